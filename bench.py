@@ -1,0 +1,403 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 space-charge FMM (FMMB200) on the N = 2^24 Gaussian bunch.
+
+A step is one field evaluation -- update_particles_field!(beam, FMMB200(0.5, 125, 4);
+lambda=1) from positions/momenta to E and B -- over the whole synthetic beam:
+tree build, traversal, P2M/M2M, M2L, P2P, L2L/L2P.
+
+  value    mixed (FP32 arithmetic, FP64 geometry) form, particles/s with the
+           inputs resident in HBM (device-pointer C-ABI call)
+  fp64     the plain FP64 path on the same inputs
+  e2e      the mixed form through the host-pointer C-ABI (the call the drop-in
+           makes): pinned host inputs copied in and fields copied out every step
+  roofline the dominant kernel (M2L) against the measured CUDA-core FMA peak
+  accuracy rel-L2 of mixed vs FP64 over all particles, and of both vs an FP64
+           direct sum (GPU) on 4096 seeded targets
+
+--impl reference times the reference's algorithm on the host cores: the
+oracle's restatement of the serial FMM (parallel over targets with OpenMP,
+bit-identical to serial) on a bounded sample of the same workload.
+
+Multi-GPU (--gpus N under torchrun): the field evaluation is replicated, one
+independent beam per rank (weak scaling); the timing is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "fmm4rbgpu.jl_b200"))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "particles/s at N=2^24: FP32 form vs FP64 plain at stated rel err; fwd+bwd time"
+SM_COUNT_NOTE = "B200, 148 SMs"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--N", type=int, default=2**24)
+    ap.add_argument("--n", type=int, default=4)
+    ap.add_argument("--N0", type=int, default=125)
+    ap.add_argument("--eta", type=float, default=0.5)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--ntargets", type=int, default=4096)
+    ap.add_argument("--cpu-sample", type=int, default=2**17, help="particles in the CPU-baseline sample")
+    ap.add_argument("--ref-sample", type=int, default=2**18, help="particles per reference-arm step")
+    ap.add_argument("--skip-cpu-baseline", action="store_true")
+    ap.add_argument("--skip-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def workload(args):
+    return {
+        "workload": f"Gaussian bunch N={args.N} (sigma=(1,1,0.1), u_z~N(200,0.2), u_x,u_y~N(0,0.01)), "
+                    f"n={args.n}, N0={args.N0}, eta={args.eta}, lambda=1; value = mixed form, fp64 = plain path",
+        "npar": args.N, "n": args.n, "N0": args.N0, "eta": args.eta, "lambda": 1.0,
+        "l2": "inputs larger than L2 (AoS positions+momenta 48 B/particle resident in HBM; no flush)",
+    }
+
+
+# ---------------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during a region."""
+
+    FIELDS = ("uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid: str | None):
+        self.uuid = uuid
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        rows = []
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            if self.uuid and f[0] != self.uuid:
+                continue
+            try:
+                rows.append(dict(sm=float(f[1]), smax=float(f[2]), power=float(f[3]), hw=f[5], hwt=f[6], swt=f[7],
+                                 swp=f[8]))
+            except ValueError:
+                continue
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        load = [r for r in rows if r["power"] > 300.0] or rows
+        reasons = set()
+        for r in load:
+            for key, name in (("hw", "hw_slowdown"), ("hwt", "hw_thermal_slowdown"), ("swt", "sw_thermal_slowdown"),
+                              ("swp", "sw_power_cap")):
+                if r[key].lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(r["sm"] for r in load), "sm_max_mhz": max(r["smax"] for r in rows),
+                "reasons": sorted(reasons), "samples": len(load), "power_w_max": max(r["power"] for r in rows)}
+
+
+# ---------------------------------------------------------------------------- helpers
+def model_flops(st: dict, n: int, N: int) -> float:
+    """Algorithmic flop count: 41 per kernel evaluation plus the interpolation terms
+    (the reference's dense M2M/L2L counts)."""
+    M = n + 1
+    NN = M ** 3
+    nc = st["ncluster"]
+    return (41.0 * (st["m2l_kernel_evals"] + st["p2p_kernel_evals"]) + N * (10 * NN + 12 * M + 6)
+            + N * (14 * NN + 12 * M) + 10.0 * NN * NN * (nc - 1) + 14.0 * NN * NN * (nc - 1))
+
+
+def dist_setup(args):
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(world, v: float) -> float:
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------- reference arm
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    import oracle
+    from fmmb200 import beams
+
+    nthreads = os.cpu_count() or 1
+    N = min(args.ref_sample, args.N)
+    pos, mom = beams.gaussian_bunch(N, seed=args.seed)
+    for _ in range(args.warmup):
+        oracle.fmm(pos, mom, -1.0, 1.0, args.n, args.N0, args.eta, nthreads=nthreads)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        oracle.fmm(pos, mom, -1.0, 1.0, args.n, args.N0, args.eta, nthreads=nthreads)
+        times.append(time.perf_counter() - t0)
+    t = sum(times) / len(times)
+    v = N / t
+    sample = (f"one FMM field evaluation of a {N}-particle Gaussian bunch (same distribution, n, N0, eta) per step; "
+              f"the oracle's restatement of the reference's serial FMM (src/fmm/*.jl), OpenMP over targets")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "particles/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Gaussian bunch)",
+        "config": workload(args),
+        "cpu_baseline": {"value": v, "unit": "particles/s", "cores": nthreads, "kind": "port", "sample": sample},
+        "e2e": {"value": v, "unit": "particles/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def cpu_baseline(args):
+    import oracle
+    from fmmb200 import beams
+
+    N = min(args.cpu_sample, args.N)
+    pos, mom = beams.gaussian_bunch(N, seed=args.seed + 1)
+    t0 = time.perf_counter()
+    oracle.fmm(pos, mom, -1.0, 1.0, args.n, args.N0, args.eta, nthreads=1)
+    t = time.perf_counter() - t0
+    return {"value": N / t, "unit": "particles/s", "cores": 1, "kind": "port",
+            "sample": f"one serial FMM field evaluation (the oracle's restatement of src/fmm/*.jl, 1 thread) of a "
+                      f"{N}-particle Gaussian bunch with the same distribution, n, N0 and eta; {t:.1f} s"}
+
+
+# ---------------------------------------------------------------------------- our arm
+def run_ours(args, world, rank, local):
+    import torch
+
+    import fmmb200
+    from fmmb200 import beams
+
+    dev = torch.device("cuda", local)
+    N = args.N
+    pos_h, mom_h = beams.gaussian_bunch(N, seed=args.seed + rank)
+    pos = torch.from_numpy(pos_h).to(dev)
+    mom = torch.from_numpy(mom_h).to(dev)
+    E = torch.empty_like(pos)
+    B = torch.empty_like(pos)
+    E64 = torch.empty_like(pos)
+    B64 = torch.empty_like(pos)
+    stream = torch.cuda.Stream(device=dev)
+    ctx = fmmb200.Context(local)
+    ctx.set_stream(stream.cuda_stream)
+    ctx.set_timing(True)
+    L = ctx._lib
+    alg_mixed = fmmb200.FMMB200(n=args.n, N0=args.N0, eta=args.eta, precision="mixed")
+    alg_fp64 = fmmb200.FMMB200(n=args.n, N0=args.N0, eta=args.eta, precision="fp64")
+
+    def step(alg, e, b):
+        ctx.forward_device(N, pos.data_ptr(), mom.data_ptr(), e.data_ptr(), b.data_ptr(), alg)
+
+    def timed(alg, e, b, steps, warmup):
+        for _ in range(warmup):
+            step(alg, e, b)
+        stream.synchronize()
+        barrier(world)
+        torch.cuda.synchronize(dev)
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        stage = []
+        ev0.record(stream)
+        for _ in range(steps):
+            step(alg, e, b)
+            stage.append(ctx.stats())
+        ev1.record(stream)
+        ev1.synchronize()
+        torch.cuda.synchronize(dev)
+        barrier(world)
+        ms = ev0.elapsed_time(ev1) / steps
+        return max_over_ranks(world, ms), stage
+
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    except Exception:
+        pass
+    with ClockSampler(uuid) as clk:
+        ms_mixed, st_mixed = timed(alg_mixed, E, B, args.steps, args.warmup)
+        ms_fp64, st_fp64 = timed(alg_fp64, E64, B64, args.steps, args.warmup)
+    clocks = clk.summary()
+
+    st = st_mixed[-1]
+    st64 = st_fp64[-1]
+    # accuracy: mixed vs fp64 (all particles), both vs an FP64 direct sum on seeded targets
+    rel_e = float(torch.linalg.norm(E - E64) / torch.linalg.norm(E64))
+    rel_b = float(torch.linalg.norm(B - B64) / torch.linalg.norm(B64))
+    tg = torch.from_numpy(np.random.default_rng(args.seed + 100).choice(N, size=min(args.ntargets, N),
+                                                                          replace=False).astype(np.int64)).to(dev)
+    Ed = torch.empty((tg.numel(), 3), dtype=torch.float64, device=dev)
+    Bd = torch.empty_like(Ed)
+    st_ = L.fmmb200_direct_device(ctx.handle, N, ctypes.c_void_p(pos.data_ptr()), ctypes.c_void_p(mom.data_ptr()),
+                                  -1.0, 1.0, tg.numel(), ctypes.c_void_p(tg.data_ptr()),
+                                  ctypes.c_void_p(Ed.data_ptr()), ctypes.c_void_p(Bd.data_ptr()))
+    ctx._check(st_)
+    stream.synchronize()
+
+    def rel(a, b):
+        return float(torch.linalg.norm(a - b) / torch.linalg.norm(b))
+
+    acc = {"mixed_vs_fp64": {"E": rel_e, "B": rel_b},
+           "fp64_vs_direct": {"E": rel(E64[tg], Ed), "B": rel(B64[tg], Bd)},
+           "mixed_vs_direct": {"E": rel(E[tg], Ed), "B": rel(B[tg], Bd)},
+           "direct_targets": int(tg.numel())}
+
+    # roofline of the dominant kernel (M2L) against the measured CUDA-core FMA peak
+    p64 = ctypes.c_double()
+    p32 = ctypes.c_double()
+    ctx._check(L.fmmb200_measure_fma_peak(ctx.handle, ctypes.byref(p64), ctypes.byref(p32)))
+    m2l_flops = 41.0 * st["m2l_kernel_evals"]
+    ach32 = m2l_flops / (st["ms_m2l"] * 1e-3) / 1e12 if st["ms_m2l"] > 0 else 0.0
+    ach64 = 41.0 * st64["m2l_kernel_evals"] / (st64["ms_m2l"] * 1e-3) / 1e12 if st64["ms_m2l"] > 0 else 0.0
+    roof = {"kernel": "m2l_kernel<4, mixed>", "bound": "fp32", "achieved": ach32, "peak": p32.value,
+            "unit": "TFLOP/s", "frac": ach32 / p32.value if p32.value else None, "traffic": None,
+            "peak_source": "measured FP32 FMA throughput (fmmb200_measure_fma_peak) on this GPU",
+            "flops_per_launch": m2l_flops, "ms_per_launch": st["ms_m2l"],
+            "fp64": {"kernel": "m2l_kernel<4, fp64>", "achieved": ach64, "peak": p64.value,
+                     "frac": ach64 / p64.value if p64.value else None, "ms_per_launch": st64["ms_m2l"]}}
+
+    # end to end through the host-pointer C-ABI (pinned host buffers)
+    e2e = None
+    if not args.skip_e2e:
+        ph = torch.from_numpy(pos_h).pin_memory()
+        mh = torch.from_numpy(mom_h).pin_memory()
+        eh = torch.empty((N, 3), dtype=torch.float64).pin_memory()
+        bh = torch.empty((N, 3), dtype=torch.float64).pin_memory()
+        pd = ctypes.cast(ph.data_ptr(), ctypes.POINTER(ctypes.c_double))
+        md = ctypes.cast(mh.data_ptr(), ctypes.POINTER(ctypes.c_double))
+        ed = ctypes.cast(eh.data_ptr(), ctypes.POINTER(ctypes.c_double))
+        bd = ctypes.cast(bh.data_ptr(), ctypes.POINTER(ctypes.c_double))
+
+        def host_step():
+            ctx._check(L.fmmb200_update_particles_field(ctx.handle, N, -1.0, pd, md, ed, bd, args.n, args.N0,
+                                                        args.eta, 1.0, fmmb200.PRECISION_MIXED))
+
+        for _ in range(args.warmup):
+            host_step()
+        barrier(world)
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(args.steps):
+            host_step()
+        ev1.record(stream)
+        ev1.synchronize()
+        ms_e2e = max_over_ranks(world, ev0.elapsed_time(ev1) / args.steps)
+        assert torch.equal(eh, E.cpu()), "host-pointer and device-pointer paths must agree"
+        e2e = {"value": world * N / (ms_e2e * 1e-3), "unit": "particles/s", "ms_per_step": ms_e2e,
+               "h2d_bytes_per_step": 2 * 24 * N, "d2h_bytes_per_step": 2 * 24 * N}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.skip_cpu_baseline:
+        cpu = cpu_baseline(args)
+
+    if rank == 0:
+        stages = {k: st[k] for k in ("ms_tree", "ms_upward", "ms_lists", "ms_m2l", "ms_p2p", "ms_downward")}
+        stages64 = {k: st64[k] for k in ("ms_tree", "ms_upward", "ms_lists", "ms_m2l", "ms_p2p", "ms_downward")}
+        mf = model_flops(st, args.n, N)
+        out = {
+            "metric": METRIC, "value": world * N / (ms_mixed * 1e-3), "unit": "particles/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_mixed, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic: seeded Gaussian bunch per rank (the reference benchmarks no public dataset)",
+            "config": workload(args),
+            "fp64": {"value": world * N / (ms_fp64 * 1e-3), "unit": "particles/s", "ms_per_step": ms_fp64,
+                     "stages_ms": stages64, "mixed_speedup": ms_fp64 / ms_mixed},
+            "accuracy": acc,
+            "stages_ms": stages,
+            "work": {"nm2l": st["nm2l"], "np2p": st["np2p"], "m2l_kernel_evals": st["m2l_kernel_evals"],
+                     "p2p_kernel_evals": st["p2p_kernel_evals"], "max_level": st["max_level"],
+                     "ncluster": st["ncluster"], "model_flops_per_step": mf,
+                     "model_tflops_mixed": mf / (ms_mixed * 1e-3) / 1e12,
+                     "model_tflops_fp64": mf / (ms_fp64 * 1e-3) / 1e12, "device_bytes": st["device_bytes"]},
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": int(st["kernel_launches"]) * args.steps,
+            "clocks": clocks,
+        }
+        print(json.dumps(out), flush=True)
+    ctx.close()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        rank = int(os.environ.get("RANK", "0"))
+        run_reference(args, world, rank)
+        return
+    world, rank, local = dist_setup(args)
+    try:
+        run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

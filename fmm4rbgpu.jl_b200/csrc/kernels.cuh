@@ -1,0 +1,65 @@
+// kernels.cuh -- host-side launchers shared between the translation units.
+#pragma once
+
+#include "context.cuh"
+
+namespace fmmb200 {
+
+// Lets kernel `k` use `dyn` bytes of dynamic shared memory (static shared memory
+// counts against the same 48 KB default, so opt in whenever the sum may exceed it).
+template <class K>
+inline int opt_in_smem(Ctx *ctx, K k, int dyn) {
+  if (dyn <= 16 * 1024) return FMMB200_OK;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+  if (e != cudaSuccess) return ctx->fail(FMMB200_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+  return FMMB200_OK;
+}
+
+// ---------------------------------------------------------------- sort.cu
+// Stable LSD radix sort by key bits [0, key_bits) (8-bit digits, passes whose
+// digit is constant are skipped).  vals/vals_alt may be null (keys only).
+// On return *in_alt tells whether the sorted data is in the *_alt buffers.
+int radix_sort(Ctx *ctx, uint64_t *keys, uint64_t *keys_alt, uint32_t *vals, uint32_t *vals_alt,
+               int64_t n, int key_bits, bool *in_alt);
+// Exclusive scan of n int32 values (in and out may alias); *total (host) if not null.
+int exclusive_scan_i32(Ctx *ctx, const int *in, int *out, int64_t n, int64_t *total);
+
+// ---------------------------------------------------------------- tree.cu
+// Device p_avg with the pairwise summation structure of Julia's Base.sum and
+// stretch = (1, 1, sqrt(1 + p.p)) into d_consts[0..5].
+int compute_pavg_stretch(Ctx *ctx, const double *d_mom_aos, int64_t N, double *d_consts);
+// Build the cluster tree of N particles (AoS positions on device) with the
+// stretch in d_consts[3..5]; fills ctx tree buffers and ctx->{N,N0,ml,nc,...}.
+int build_tree(Ctx *ctx, const double *d_pos_aos, int64_t N, int64_t N0, const double *d_consts);
+// Particle records in tree order ("prec64": x,y,z,gamma,ux,uy,uz,0) and, for
+// the mixed form, leaf-local FP32 records ("prec32").
+// leafpos (optional): leaf cluster of every tree-order position (explicit trees).
+int gather_particles(Ctx *ctx, const double *d_pos_aos, const double *d_mom_aos, bool mixed,
+                     const int *leafpos = nullptr);
+// Traversal geometry (centre, radius, diameter, leaf flag) for the stretch in d_consts[3..5].
+int compute_geom(Ctx *ctx, const double *d_consts);
+// Chebyshev node coordinates (degree n) of every cluster into "nodes".
+int compute_nodes(Ctx *ctx, int n);
+int node_stride(int n);
+
+// ---------------------------------------------------------------- traverse.cu
+int build_lists(Ctx *ctx, double eta, const double *d_consts);
+
+// ---------------------------------------------------------------- interp.cu
+// P2M of leaves (leaf_ids null: all leaves of the tree) into "mom"; accumulate
+// adds to the existing moments instead of overwriting them.
+int launch_p2m(Ctx *ctx, int n, bool mixed, const int *d_leaf_ids, int64_t nleaf, bool accumulate);
+// M2M for all parents at parent level `plevel` (children at plevel+1).
+int launch_m2m(Ctx *ctx, int n, bool mixed, int plevel, bool accumulate);
+// L2L for all children at child level `clevel` (>= 1).
+int launch_l2l(Ctx *ctx, int n, bool mixed, int clevel);
+// L2P of leaves.  mode 0: explicit (near += far at tree-order particles);
+// mode 1: pipeline (out_aos[perm] = amp * (near + far)).
+int launch_l2p(Ctx *ctx, int n, bool mixed, const int *d_leaf_ids, int64_t nleaf, int mode,
+               double amp, double *d_out_e, double *d_out_b);
+
+// ---------------------------------------------------------------- m2l.cu / p2p.cu
+int launch_m2l(Ctx *ctx, int n, bool mixed, bool accumulate);
+int launch_p2p(Ctx *ctx, bool mixed, const int *d_leaf_ids, int64_t nleaf, bool accumulate);
+
+}  // namespace fmmb200

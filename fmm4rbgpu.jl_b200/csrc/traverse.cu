@@ -1,0 +1,283 @@
+// traverse.cu -- device dual-tree traversal (the reference's dualtraversefill!,
+// src/fmm/interaction_lists.jl:23-49, a host recursion there) and the CSR
+// grouping by target (InteractionListsGPU, src/gpu_fmm/gpu_interaction_lists.jl:27-40).
+//
+// Design: a breadth-first traversal over frontiers of (target, source) pairs.
+// Each step classifies every frontier pair with the reference's rules (both
+// leaves -> P2P; admissible -> M2L; otherwise split the non-leaf side, or the
+// side with the larger stretched diameter, ties to the source) and writes its
+// outputs at offsets from a block scan, so every step is deterministic.  The
+// set of emitted pairs equals the DFS's.  Both lists are then radix-sorted by
+// (target, source) and grouped into CSR pointers over all clusters.
+#include "device_util.cuh"
+#include "kernels.cuh"
+
+namespace fmmb200 {
+
+namespace {
+
+constexpr int kTvThreads = 256;
+constexpr int kTvItems = 4;
+constexpr int kTvTile = kTvThreads * kTvItems;
+
+enum : int { kCatP2P = 0, kCatM2L = 1, kCatSplit = 2 };
+
+// Returns the category; for a split, (*ct1,*cs1),(*ct2,*cs2) are the child pairs.
+__device__ __forceinline__ int classify(const ClusterGeom *__restrict__ geom, int t, int s, double s0, double s1,
+                                        double s2, double eta, int *ct1, int *cs1, int *ct2, int *cs2) {
+  const ClusterGeom gt = geom[t], gs = geom[s];
+  if (gt.leaf && gs.leaf) return kCatP2P;
+  // admissible(): max(r1,r2)/R < eta with R = norm(stretch .* (xc1 - xc2))
+  double R = norm3_exact(rn_mul(s0, rn_sub(gt.xc[0], gs.xc[0])), rn_mul(s1, rn_sub(gt.xc[1], gs.xc[1])),
+                         rn_mul(s2, rn_sub(gt.xc[2], gs.xc[2])));
+  double m = gt.r > gs.r ? gt.r : gs.r;
+  if (__ddiv_rn(m, R) < eta) return kCatM2L;
+  bool split_t;
+  if (gt.leaf)
+    split_t = false;
+  else if (gs.leaf)
+    split_t = true;
+  else
+    split_t = gt.diam > gs.diam;
+  if (split_t) {
+    *ct1 = 2 * t + 1;
+    *cs1 = s;
+    *ct2 = 2 * t + 2;
+    *cs2 = s;
+  } else {
+    *ct1 = t;
+    *cs1 = 2 * s + 1;
+    *ct2 = t;
+    *cs2 = 2 * s + 2;
+  }
+  return kCatSplit;
+}
+
+__global__ void trav_count_kernel(const int2 *__restrict__ front, int nf, const ClusterGeom *__restrict__ geom,
+                                  const double *__restrict__ consts, double eta, int nblk,
+                                  int *__restrict__ bcount, int *__restrict__ totals) {
+  __shared__ int s_warp[33];
+  const double s0 = consts[3], s1 = consts[4], s2 = consts[5];
+  int c[3] = {0, 0, 0};
+  int i0 = blockIdx.x * kTvTile + threadIdx.x * kTvItems;
+  for (int i = 0; i < kTvItems; ++i) {
+    int q = i0 + i;
+    if (q < nf) {
+      int2 p = front[q];
+      int a, b, cc, d;
+      c[classify(geom, p.x, p.y, s0, s1, s2, eta, &a, &b, &cc, &d)]++;
+    }
+  }
+  for (int k = 0; k < 3; ++k) {
+    int tot;
+    block_excl_scan(c[k], s_warp, &tot);
+    if (threadIdx.x == 0) {
+      bcount[k * nblk + blockIdx.x] = tot;
+      if (tot) atomicAdd(&totals[k], tot);
+    }
+  }
+}
+
+__global__ void trav_write_kernel(const int2 *__restrict__ front, int nf, const ClusterGeom *__restrict__ geom,
+                                  const double *__restrict__ consts, double eta, int nblk,
+                                  const int *__restrict__ boff, int bits, uint64_t *__restrict__ p2p,
+                                  uint64_t *__restrict__ m2l, int2 *__restrict__ next) {
+  __shared__ int s_warp[33];
+  const double s0 = consts[3], s1 = consts[4], s2 = consts[5];
+  int cat[kTvItems];
+  int2 pr[kTvItems], ch1[kTvItems], ch2[kTvItems];
+  int c[3] = {0, 0, 0};
+  int i0 = blockIdx.x * kTvTile + threadIdx.x * kTvItems;
+  for (int i = 0; i < kTvItems; ++i) {
+    int q = i0 + i;
+    cat[i] = -1;
+    if (q < nf) {
+      pr[i] = front[q];
+      cat[i] = classify(geom, pr[i].x, pr[i].y, s0, s1, s2, eta, &ch1[i].x, &ch1[i].y, &ch2[i].x, &ch2[i].y);
+      c[cat[i]]++;
+    }
+  }
+  int pos[3];
+  for (int k = 0; k < 3; ++k)
+    pos[k] = block_excl_scan(c[k], s_warp, nullptr) + boff[k * nblk + blockIdx.x] - boff[k * nblk];
+  for (int i = 0; i < kTvItems; ++i) {
+    if (cat[i] < 0) continue;
+    uint64_t key = ((uint64_t)pr[i].x << bits) | (uint64_t)pr[i].y;
+    if (cat[i] == kCatP2P) {
+      p2p[pos[0]++] = key;
+    } else if (cat[i] == kCatM2L) {
+      m2l[pos[1]++] = key;
+    } else {
+      int o = pos[2]++;
+      next[2 * o] = ch1[i];
+      next[2 * o + 1] = ch2[i];
+    }
+  }
+}
+
+// ptr[c] = first list position with target c (lists sorted by key), src[i] = source.
+__global__ void csr_kernel(const uint64_t *__restrict__ keys, int64_t n, int bits, int64_t nc,
+                           int *__restrict__ ptr) {
+  int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c > nc) return;
+  uint64_t want = (uint64_t)c << bits;
+  int64_t lo = 0, hi = n;
+  while (lo < hi) {
+    int64_t mid = (lo + hi) >> 1;
+    if (keys[mid] < want)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  ptr[c] = (int)lo;
+}
+
+__global__ void src_kernel(const uint64_t *__restrict__ keys, int64_t n, int bits, int *__restrict__ src) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  src[i] = (int)(keys[i] & (((uint64_t)1 << bits) - 1));
+}
+
+__global__ void p2p_work_kernel(const uint64_t *__restrict__ keys, int64_t n, int bits, const int *__restrict__ lohi,
+                                unsigned long long *__restrict__ out) {
+  __shared__ unsigned long long s;
+  if (threadIdx.x == 0) s = 0;
+  __syncthreads();
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long w = 0;
+  if (i < n) {
+    uint64_t k = keys[i];
+    int t = (int)(k >> bits), sc = (int)(k & (((uint64_t)1 << bits) - 1));
+    w = (unsigned long long)(lohi[2 * t + 1] - lohi[2 * t] + 1) * (unsigned long long)(lohi[2 * sc + 1] - lohi[2 * sc] + 1);
+  }
+  w = warp_sum(w);
+  if ((threadIdx.x & 31) == 0 && w) atomicAdd(&s, w);
+  __syncthreads();
+  if (threadIdx.x == 0 && s) atomicAdd(out, s);
+}
+
+// Grow a device buffer keeping its first `used` bytes.
+int grow_keep(Ctx *ctx, const char *name, size_t used, size_t need, void **out) {
+  auto it = ctx->bufs.find(name);
+  if (it != ctx->bufs.end() && it->second.cap >= need) {
+    *out = it->second.p;
+    return FMMB200_OK;
+  }
+  void *fresh = nullptr;
+  size_t want = need + need / 2;
+  want = (want + 255) & ~(size_t)255;
+  if (ctx->fail_alloc_countdown > 0 && --ctx->fail_alloc_countdown == 0)
+    return ctx->fail(FMMB200_ERR_OUT_OF_MEMORY, std::string("injected allocation failure for buffer '") + name + "'");
+  cudaError_t e = cudaMalloc(&fresh, want);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return ctx->fail(FMMB200_ERR_OUT_OF_MEMORY, std::string("cudaMalloc for '") + name + "': " + cudaGetErrorString(e));
+  }
+  if (it != ctx->bufs.end() && it->second.p) {
+    if (used) FMM_CUDA_TRY(ctx, cudaMemcpyAsync(fresh, it->second.p, used, cudaMemcpyDeviceToDevice, ctx->stream));
+    FMM_TRY(ctx->sync());
+    cudaFree(it->second.p);
+    ctx->device_bytes -= it->second.cap;
+  }
+  auto &b = ctx->bufs[name];
+  b.p = fresh;
+  b.cap = want;
+  ctx->device_bytes += want;
+  *out = fresh;
+  return FMMB200_OK;
+}
+
+int sort_and_group(Ctx *ctx, const char *keys_name, const char *alt_name, const char *ptr_name,
+                   const char *src_name, int64_t n, int bits) {
+  uint64_t *keys = ctx->get<uint64_t>(keys_name), *alt = nullptr;
+  FMM_TRY(ctx->ensure(alt_name, n, &alt));
+  keys = ctx->get<uint64_t>(keys_name);
+  bool in_alt = false;
+  FMM_TRY(radix_sort(ctx, keys, alt, nullptr, nullptr, n, 2 * bits, &in_alt));
+  if (in_alt) std::swap(ctx->bufs[keys_name], ctx->bufs[alt_name]);
+  keys = ctx->get<uint64_t>(keys_name);
+  int *ptr, *src;
+  FMM_TRY(ctx->ensure(ptr_name, ctx->nc + 1, &ptr));
+  FMM_TRY(ctx->ensure(src_name, n, &src));
+  csr_kernel<<<ceil_div(ctx->nc + 1, 256), 256, 0, ctx->stream>>>(keys, n, bits, ctx->nc, ptr);
+  if (n > 0) src_kernel<<<ceil_div(n, 256), 256, 0, ctx->stream>>>(keys, n, bits, src);
+  return ctx->check_launch("sort_and_group", n > 0 ? 2 : 1);
+}
+
+}  // namespace
+
+int build_lists(Ctx *ctx, double eta, const double *d_consts) {
+  const int64_t nc = ctx->nc;
+  FMM_TRY(compute_geom(ctx, d_consts));
+  int bits = 1;
+  while (((int64_t)1 << bits) < nc) ++bits;
+  int64_t cap_p = 64 * ctx->nleaf + 1024, cap_m = 32 * nc + 1024;
+  int2 *fa, *fb;
+  uint64_t *p2p, *m2l;
+  FMM_TRY(ctx->ensure("front_a", 4 * nc + 1024, &fa));
+  FMM_TRY(ctx->ensure("front_b", 4 * nc + 1024, &fb));
+  void *vp;
+  FMM_TRY(grow_keep(ctx, "p2p_keys", 0, sizeof(uint64_t) * cap_p, &vp));
+  FMM_TRY(grow_keep(ctx, "m2l_keys", 0, sizeof(uint64_t) * cap_m, &vp));
+  int *bcount, *boff, *totals;
+  int *h = nullptr;
+  FMM_TRY(ctx->ensure("trav_totals", 4, &totals));
+  int2 root = make_int2(0, 0);
+  FMM_CUDA_TRY(ctx, cudaMemcpyAsync(fa, &root, sizeof(int2), cudaMemcpyHostToDevice, ctx->stream));
+  int64_t nf = 1, np2p = 0, nm2l = 0;
+  int steps = 0;
+  const ClusterGeom *geom = ctx->get<ClusterGeom>("geom");
+  while (nf > 0) {
+    const int nblk = ceil_div(nf, kTvTile);
+    FMM_TRY(ctx->ensure("trav_bcount", 3 * (int64_t)nblk, &bcount));
+    FMM_TRY(ctx->ensure("trav_boff", 3 * (int64_t)nblk, &boff));
+    FMM_CUDA_TRY(ctx, cudaMemsetAsync(totals, 0, sizeof(int) * 4, ctx->stream));
+    trav_count_kernel<<<nblk, kTvThreads, 0, ctx->stream>>>(fa, (int)nf, geom, d_consts, eta, nblk, bcount, totals);
+    FMM_TRY(ctx->check_launch("trav_count_kernel"));
+    FMM_TRY(exclusive_scan_i32(ctx, bcount, boff, 3 * (int64_t)nblk, nullptr));
+    FMM_TRY(ctx->pinned(sizeof(int) * 4, (void **)&h));
+    FMM_CUDA_TRY(ctx, cudaMemcpyAsync(h, totals, sizeof(int) * 3, cudaMemcpyDeviceToHost, ctx->stream));
+    FMM_TRY(ctx->sync());
+    const int64_t tp = h[0], tm = h[1], ts = h[2];
+    FMM_TRY(grow_keep(ctx, "p2p_keys", sizeof(uint64_t) * np2p, sizeof(uint64_t) * (np2p + tp), &vp));
+    p2p = (uint64_t *)vp;
+    FMM_TRY(grow_keep(ctx, "m2l_keys", sizeof(uint64_t) * nm2l, sizeof(uint64_t) * (nm2l + tm), &vp));
+    m2l = (uint64_t *)vp;
+    FMM_TRY(ctx->ensure("front_b", 2 * ts + 1, &fb));  // destination: contents not needed
+    trav_write_kernel<<<nblk, kTvThreads, 0, ctx->stream>>>(fa, (int)nf, geom, d_consts, eta, nblk, boff, bits,
+                                                             p2p + np2p, m2l + nm2l, fb);
+    FMM_TRY(ctx->check_launch("trav_write_kernel"));
+    np2p += tp;
+    nm2l += tm;
+    nf = 2 * ts;
+    std::swap(ctx->bufs["front_a"], ctx->bufs["front_b"]);
+    fa = ctx->get<int2>("front_a");
+    fb = ctx->get<int2>("front_b");
+    ++steps;
+    if (steps > 4 * 64) return ctx->fail(FMMB200_ERR_DEVICE, "traversal did not terminate");
+  }
+  ctx->nm2l = nm2l;
+  ctx->np2p = np2p;
+  ctx->traversal_steps = steps;
+  FMM_TRY(sort_and_group(ctx, "m2l_keys", "m2l_keys_alt", "m2l_ptr", "m2l_src", nm2l, bits));
+  FMM_TRY(sort_and_group(ctx, "p2p_keys", "p2p_keys_alt", "p2p_ptr", "p2p_src", np2p, bits));
+  // exact P2P work for the stats
+  unsigned long long *d_work;
+  FMM_TRY(ctx->ensure("p2p_work", 1, &d_work));
+  FMM_CUDA_TRY(ctx, cudaMemsetAsync(d_work, 0, sizeof(unsigned long long), ctx->stream));
+  if (np2p > 0) {
+    p2p_work_kernel<<<ceil_div(np2p, 256), 256, 0, ctx->stream>>>(ctx->get<uint64_t>("p2p_keys"), np2p, bits,
+                                                                  ctx->get<int>("lohi"), d_work);
+    FMM_TRY(ctx->check_launch("p2p_work_kernel"));
+  }
+  unsigned long long *hw;
+  FMM_TRY(ctx->pinned(sizeof(unsigned long long), (void **)&hw));
+  FMM_CUDA_TRY(ctx, cudaMemcpyAsync(hw, d_work, sizeof(unsigned long long), cudaMemcpyDeviceToHost, ctx->stream));
+  FMM_TRY(ctx->sync());
+  ctx->stats.p2p_kernel_evals = (double)*hw;
+  ctx->list_bits = bits;
+  ctx->have_lists = true;
+  return FMMB200_OK;
+}
+
+}  // namespace fmmb200

@@ -1,0 +1,194 @@
+"""End-to-end parity of update_particles_field!(beam, FMMB200(eta, N0, n); lambda).
+
+The plain FP64 path must match the oracle's serial FMM (src/fmm/*.jl restated)
+within 1e-12 relative L2 for E and B; every result is also checked against the
+FP64 direct sum (BruteForce).  The mixed form must stay within 1e-5 of the
+FP64 path, below the FMM's own truncation error.
+"""
+import numpy as np
+import pytest
+
+from conftest import NTHREADS
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-12
+MIXED_TOL = 1e-5
+
+
+def rel(a, b):
+    from fmmb200.beams import rel_l2
+
+    return rel_l2(a, b)
+
+
+def make(kind, N, seed):
+    from fmmb200 import beams
+
+    return {"uniform": beams.uniform, "gauss": beams.gaussian_bunch, "beamlets": beams.beamlets}[kind](N, seed=seed)
+
+
+@pytest.mark.parametrize("N,kind,n,N0", [(65536, "uniform", 4, 125), (65536, "gauss", 4, 125),
+                                         (40000, "beamlets", 5, 64), (30000, "gauss", 2, 50),
+                                         (20000, "gauss", 6, 125), (12345, "uniform", 3, 37)])
+def test_fp64_matches_oracle_fmm(gpu_ctx, oracle_mod, N, kind, n, N0):
+    import fmmb200
+
+    pos, mom = make(kind, N, 0)
+    E, B = gpu_ctx.forward(pos, mom, fmmb200.FMMB200(n=n, N0=N0, eta=0.5), charge=-1.0, lambda_=1.0)
+    Eo, Bo, st = oracle_mod.fmm(pos, mom, -1.0, 1.0, n, N0, 0.5, nthreads=NTHREADS)
+    assert rel(E, Eo) < FP64_TOL
+    if kind == "uniform":
+        assert np.all(B == 0.0) and np.all(Bo == 0.0)  # zero momenta: B is exactly zero
+    else:
+        assert rel(B, Bo) < FP64_TOL
+    i = gpu_ctx.tree_info()
+    assert (i["nm2l"], i["np2p"]) == (st["nm2l"], st["np2p"])
+
+
+def test_config1_against_bruteforce(gpu_ctx, oracle_mod):
+    """N=65,536 uniform, u=0, n=4, N0=125, eta=0.5: FMM truncation error vs BruteForce."""
+    import fmmb200
+
+    pos, mom = make("uniform", 65536, 0)
+    E, B = gpu_ctx.forward(pos, mom, fmmb200.FMMB200(n=4, N0=125, eta=0.5))
+    Eb, Bb = oracle_mod.bruteforce(pos, mom, -1.0, 1.0, NTHREADS)
+    assert rel(E, Eb) < 5e-3
+    assert np.all(B == 0.0) and np.all(Bb == 0.0)
+
+
+def test_mixed_matches_fp64(gpu_ctx):
+    import fmmb200
+
+    pos, mom = make("gauss", 2**17, 2)
+    E, B = gpu_ctx.forward(pos, mom, fmmb200.FMMB200(n=4, N0=125, eta=0.5))
+    Em, Bm = gpu_ctx.forward(pos, mom, fmmb200.FMMB200(n=4, N0=125, eta=0.5, precision="mixed"))
+    assert rel(Em, E) < MIXED_TOL and rel(Bm, B) < MIXED_TOL
+
+
+def test_update_particles_field_overwrites(gpu_ctx, oracle_mod):
+    import fmmb200
+
+    pos, mom = make("gauss", 5000, 3)
+    p = fmmb200.Particles(pos=pos.T, mom=mom.T, charge=-1.0)
+    p.efields[...] = 123.0
+    alg = fmmb200.FMMB200.positional(0.5, 64, 4)
+    gpu_ctx.update_particles_field(p, alg, lambda_=2.0)
+    E1 = p.efields.copy()
+    gpu_ctx.update_particles_field(p, alg, lambda_=2.0)  # second call: same fields (no accumulation)
+    assert np.array_equal(E1, p.efields)
+    Eo, Bo, _ = oracle_mod.fmm(pos, mom, -1.0, 2.0, 4, 64, 0.5, nthreads=NTHREADS)
+    assert rel(p.efields, Eo) < FP64_TOL and rel(p.bfields, Bo) < FP64_TOL
+    np.testing.assert_array_equal(p.positions, pos)  # inputs unchanged
+
+
+def test_deterministic(gpu_ctx):
+    import fmmb200
+
+    pos, mom = make("beamlets", 50000, 4)
+    alg = fmmb200.FMMB200(n=4, N0=64, eta=0.5)
+    a = gpu_ctx.forward(pos, mom, alg)
+    b = gpu_ctx.forward(pos, mom, alg)
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+
+
+@pytest.mark.parametrize("N,N0", [(1, 125), (2, 125), (100, 200), (125, 125)])
+def test_single_leaf_equals_direct_sum(gpu_ctx, oracle_mod, N, N0):
+    import fmmb200
+
+    pos, mom = make("gauss", N, 5)
+    E, B = gpu_ctx.forward(pos, mom, fmmb200.FMMB200(n=4, N0=N0, eta=0.5))
+    Eb, Bb = oracle_mod.bruteforce(pos, mom, -1.0, 1.0, 1)
+    if N == 1:
+        assert np.all(E == 0.0) and np.all(B == 0.0)
+    else:
+        assert rel(E, Eb) < 1e-13 and rel(B, Bb) < 1e-13
+
+
+def test_given_pavg_is_used(gpu_ctx, oracle_mod):
+    import fmmb200
+
+    pos, mom = make("gauss", 20000, 6)
+    pa = np.array([0.0, 0.0, 199.9])
+    E, B = gpu_ctx.forward(pos, mom, fmmb200.FMMB200(n=3, N0=80, eta=0.5), p_avg=pa)
+    Eo, Bo, _ = oracle_mod.fmm(pos, mom, -1.0, 1.0, 3, 80, 0.5, p_avg=pa, nthreads=NTHREADS)
+    assert rel(E, Eo) < FP64_TOL and rel(B, Bo) < FP64_TOL
+    st = gpu_ctx.stats()
+    assert st["pavg"] == pa.tolist()
+
+
+def test_device_pavg_matches_pairwise_sum(gpu_ctx, oracle_mod):
+    import fmmb200
+
+    for N in (1, 7, 15, 16, 1024, 1025, 5000, 2**17 + 3):
+        pos, mom = make("gauss", N, 9)
+        gpu_ctx.forward(pos, mom, fmmb200.FMMB200(n=2, N0=100, eta=0.5))
+        st = gpu_ctx.stats()
+        assert st["pavg"] == oracle_mod.pavg(mom).tolist(), N
+        assert st["stretch"] == oracle_mod.stretch(oracle_mod.pavg(mom)).tolist(), N
+
+
+def test_errors_are_statuses(gpu_ctx):
+    import fmmb200
+
+    pos, mom = make("uniform", 251, 0)
+    with pytest.raises(fmmb200.FMMB200Error) as ei:  # a leaf would sit above the max level
+        gpu_ctx.forward(pos, mom, fmmb200.FMMB200(n=4, N0=125, eta=0.5))
+    assert ei.value.status == fmmb200.ERR_TREE_SHAPE
+    pos, mom = make("uniform", 1000, 0)
+    bad = pos.copy()
+    bad[17, 1] = np.nan
+    with pytest.raises(fmmb200.FMMB200Error) as ei:
+        gpu_ctx.forward(bad, mom, fmmb200.FMMB200(n=4, N0=125, eta=0.5))
+    assert ei.value.status == fmmb200.ERR_INVALID_ARGUMENT
+    for n in (0, 11):
+        with pytest.raises(fmmb200.FMMB200Error) as ei:
+            gpu_ctx.forward(pos, mom, fmmb200.FMMB200(n=n, N0=125, eta=0.5))
+        assert ei.value.status == fmmb200.ERR_INVALID_ARGUMENT
+    with pytest.raises(fmmb200.FMMB200Error):
+        gpu_ctx.forward(pos, mom, fmmb200.FMMB200(n=4, N0=0, eta=0.5))
+    # the context still works afterwards
+    E, _ = gpu_ctx.forward(pos, mom, fmmb200.FMMB200(n=4, N0=125, eta=0.5))
+    assert np.all(np.isfinite(E))
+
+
+def test_injected_allocation_failure(gpu_ctx):
+    import fmmb200
+
+    ctx = fmmb200.Context(0)
+    pos, mom = make("gauss", 3000, 1)
+    ctx.debug_fail_alloc(3)
+    with pytest.raises(fmmb200.FMMB200Error) as ei:
+        ctx.forward(pos, mom, fmmb200.FMMB200(n=4, N0=64, eta=0.5))
+    assert ei.value.status == fmmb200.ERR_OUT_OF_MEMORY
+    E, _ = ctx.forward(pos, mom, fmmb200.FMMB200(n=4, N0=64, eta=0.5))
+    E2, _ = gpu_ctx.forward(pos, mom, fmmb200.FMMB200(n=4, N0=64, eta=0.5))
+    assert np.array_equal(E, E2)
+    ctx.close()
+
+
+def test_context_reuse_across_sizes(gpu_ctx, oracle_mod):
+    import fmmb200
+
+    for N, n in ((30000, 4), (3000, 3), (70000, 2)):
+        pos, mom = make("gauss", N, N)
+        E, B = gpu_ctx.forward(pos, mom, fmmb200.FMMB200(n=n, N0=100, eta=0.5))
+        Eo, Bo, _ = oracle_mod.fmm(pos, mom, -1.0, 1.0, n, 100, 0.5, nthreads=NTHREADS)
+        assert rel(E, Eo) < FP64_TOL and rel(B, Bo) < FP64_TOL
+
+
+def test_tree_and_lists_after_forward_match_oracle(gpu_ctx, oracle_mod):
+    import fmmb200
+
+    pos, mom = make("gauss", 65536, 12)
+    gpu_ctx.forward(pos, mom, fmmb200.FMMB200(n=4, N0=125, eta=0.5))
+    t = gpu_ctx.tree()
+    stretch = oracle_mod.stretch(oracle_mod.pavg(mom))
+    ref = oracle_mod.cluster_tree(pos, 125, stretch)
+    np.testing.assert_array_equal(t["parindices"], ref["parindices"])
+    np.testing.assert_array_equal(t["parlohis"], ref["parlohis"])
+    assert np.array_equal(t["bboxes"], ref["bboxes"])
+    m2l, p2p = gpu_ctx.lists()
+    rp2p, rm2l = oracle_mod.interaction_lists(ref["children"], ref["bboxes"], stretch, 0.5)
+    np.testing.assert_array_equal(m2l, rm2l[np.lexsort((rm2l[:, 1], rm2l[:, 0]))])
+    np.testing.assert_array_equal(p2p, rp2p[np.lexsort((rp2p[:, 1], rp2p[:, 0]))])
