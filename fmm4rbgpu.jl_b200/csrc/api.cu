@@ -45,6 +45,11 @@ __global__ void finite_check_kernel(const double *__restrict__ a, int64_t n, int
   if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicExch(flag, 1);
 }
 
+__global__ void widen_kernel(const float *__restrict__ a, int64_t n, double *__restrict__ b) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    b[i] = (double)a[i];
+}
+
 // stretch = (1, 1, sqrt(1 + p.p)) for a caller-given p_avg (update_particles_field.jl:46-47)
 __global__ void stretch_kernel(double *__restrict__ consts) {
   const double p0 = consts[0], p1 = consts[1], p2 = consts[2];
@@ -113,6 +118,7 @@ int run_forward(Ctx *ctx, int64_t N, const double *d_pos, const double *d_mom, d
   } else {
     FMM_TRY(compute_pavg_stretch(ctx, d_mom, N, consts));
   }
+  ctx->pavg_from_momenta = pavg_host == nullptr;
   FMM_TRY(build_tree(ctx, d_pos, N, N0, consts));
   FMM_TRY(gather_particles(ctx, d_pos, d_mom, mixed));
   FMM_TRY(compute_nodes(ctx, n));
@@ -680,6 +686,7 @@ int fmmb200_m2l(fmmb200_ctx *ctx, int32_t n, int32_t precision, int64_t nc, cons
   const int64_t NN = (int64_t)(n + 1) * (n + 1) * (n + 1);
   FMM_TRY(setup_clusters(ctx, n, nc, nullptr, bboxes));
   FMM_TRY(setup_pairs(ctx, "m2l", npairs, pairs));
+  ctx->eta = INFINITY;  // arbitrary pairs: target and source nodes may coincide
   double *consts;
   FMM_TRY(ctx->ensure("consts", 8, &consts));
   double c[8] = {pavg[0], pavg[1], pavg[2], 1, 1, 1, 0, 0};
@@ -819,16 +826,50 @@ int fmmb200_l2p(fmmb200_ctx *ctx, int32_t n, int32_t precision, int64_t npar, co
   return ctx->sync();
 }
 
-int fmmb200_backward(fmmb200_ctx *ctx, const double *, const double *, double *, double *) {
+int fmmb200_backward_device(fmmb200_ctx *ctx, const double *d_ge, const double *d_gb, double *d_gx,
+                            double *d_gu) {
   if (!ctx) return FMMB200_ERR_INVALID_ARGUMENT;
-  if (!ctx->saved) return ctx->fail(FMMB200_ERR_NO_STATE, "no forward saved for backward (save_for_backward=1)");
-  return ctx->fail(FMMB200_ERR_INVALID_ARGUMENT, "backward not available in this build");
+  if (!ctx->saved || !ctx->have_forward)
+    return ctx->fail(FMMB200_ERR_NO_STATE, "no forward saved for backward (call forward with save_for_backward=1)");
+  if (!d_ge || !d_gb || !d_gx || !d_gu) return ctx->fail(FMMB200_ERR_INVALID_ARGUMENT, "null pointer argument");
+  Guard g(ctx);
+  mark(ctx, kEvBwd0);
+  if (ctx->precision == FMMB200_PRECISION_MIXED) {
+    // the adjoint runs in FP64 on the saved FP32 expansions
+    const int64_t NN = (int64_t)(ctx->n + 1) * (ctx->n + 1) * (ctx->n + 1);
+    double *m64, *l64;
+    FMM_TRY(ctx->ensure("mom64", 4 * NN * ctx->nc, &m64));
+    FMM_TRY(ctx->ensure("loc64", 6 * NN * ctx->nc, &l64));
+    widen_kernel<<<592, 256, 0, ctx->stream>>>(ctx->get<float>("mom32"), 4 * NN * ctx->nc, m64);
+    widen_kernel<<<592, 256, 0, ctx->stream>>>(ctx->get<float>("loc32"), 6 * NN * ctx->nc, l64);
+    FMM_TRY(ctx->check_launch("widen_kernel", 2));
+  }
+  FMM_TRY(build_union_lists(ctx));
+  FMM_TRY(run_backward(ctx, d_ge, d_gb, d_gx, d_gu));
+  mark(ctx, kEvBwd1);
+  FMM_TRY(ctx->check_device_status("backward"));
+  if (ctx->timing) ctx->stats.ms_backward = ev_ms(ctx, kEvBwd0, kEvBwd1);
+  return FMMB200_OK;
 }
 
-int fmmb200_backward_device(fmmb200_ctx *ctx, const double *, const double *, double *, double *) {
+int fmmb200_backward(fmmb200_ctx *ctx, const double *ge, const double *gb, double *gx, double *gu) {
   if (!ctx) return FMMB200_ERR_INVALID_ARGUMENT;
-  if (!ctx->saved) return ctx->fail(FMMB200_ERR_NO_STATE, "no forward saved for backward (save_for_backward=1)");
-  return ctx->fail(FMMB200_ERR_INVALID_ARGUMENT, "backward not available in this build");
+  if (!ge || !gb || !gx || !gu) return ctx->fail(FMMB200_ERR_INVALID_ARGUMENT, "null pointer argument");
+  if (!ctx->saved || !ctx->have_forward)
+    return ctx->fail(FMMB200_ERR_NO_STATE, "no forward saved for backward (call forward with save_for_backward=1)");
+  Guard g(ctx);
+  const int64_t N = ctx->N;
+  double *dge, *dgb, *dgx, *dgu;
+  FMM_TRY(ctx->ensure("bwd_in_ge", 3 * N, &dge));
+  FMM_TRY(ctx->ensure("bwd_in_gb", 3 * N, &dgb));
+  FMM_TRY(ctx->ensure("bwd_out_gx", 3 * N, &dgx));
+  FMM_TRY(ctx->ensure("bwd_out_gu", 3 * N, &dgu));
+  FMM_CUDA_TRY(ctx, cudaMemcpyAsync(dge, ge, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, ctx->stream));
+  FMM_CUDA_TRY(ctx, cudaMemcpyAsync(dgb, gb, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, ctx->stream));
+  FMM_TRY(fmmb200_backward_device(ctx, dge, dgb, dgx, dgu));
+  FMM_CUDA_TRY(ctx, cudaMemcpyAsync(gx, dgx, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, ctx->stream));
+  FMM_CUDA_TRY(ctx, cudaMemcpyAsync(gu, dgu, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, ctx->stream));
+  return ctx->sync();
 }
 
 }  // extern "C"

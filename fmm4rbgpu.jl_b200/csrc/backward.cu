@@ -1,0 +1,911 @@
+// backward.cu -- hand-written adjoint of the whole field map (E, B) = F(x, u)
+// with the tree and the interaction lists held fixed (no counterpart in the
+// reference; the map is piecewise smooth in x through the bounding boxes).
+//
+// Reverse of the forward pipeline, all FP64:
+//   L2P^T   leaf local adjoints  += sum_p a_p w(x_p);   x_p and leaf boxes get
+//           the derivative of the interpolant
+//   L2L^T   parent local adjoints += transferred child adjoints; child/parent
+//           boxes through the node positions (levels ml .. 1)
+//   M2L^T   per target cluster over the union of its list and its transpose:
+//           node-position gradients, source-role moment adjoints, d/dp_avg
+//   M2M^T   child moment adjoints += transferred parent adjoints; boxes (top-down)
+//   P2M^T   x_p, u_p from the leaf moment adjoints; leaf boxes
+//   P2P^T   per target leaf over the union list (near field recomputed)
+//   boxes   bounding-box adjoints flow down the tree to the extremal particles,
+//           p_avg's adjoint to every momentum, then the scatter to caller order.
+//
+// Box geometry: node i of [a, b] is a + t_i (b - a) and a Lagrange weight only
+// depends on xi = (x - a)/(b - a), so for an evaluation point x with partial G:
+// dL/da += (xi - 1) G, dL/db += -xi G; for a node of the cluster itself:
+// dL/da += (1 - t_i) G_i, dL/db += t_i G_i.
+#include <cmath>
+
+#include "device_util.cuh"
+#include "interp_util.cuh"
+#include "kernels.cuh"
+
+namespace fmmb200 {
+
+namespace {
+
+template <int NDEG>
+struct BShape {
+  static constexpr int M = NDEG + 1;
+  static constexpr int NN = M * M * M;
+  static constexpr int NS = ((3 * M) + 1) & ~1;
+  static constexpr int BT = NN <= 64 ? 64 : (NN <= 512 ? ((NN + 31) / 32) * 32 : 512);
+  static constexpr int NPT = (NN + BT - 1) / BT;
+};
+
+// block-wide sum of V doubles per thread into out (all threads get the result)
+template <int V>
+__device__ __forceinline__ void block_sum(double (&v)[V], double *s_red /* [32][V] */) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+  for (int k = 0; k < V; ++k) v[k] = warp_sum(v[k]);
+  __syncthreads();
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < V; ++k) s_red[wid * V + k] = v[k];
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < V; ++k) {
+    double s = 0.0;
+    for (int w = 0; w < nw; ++w) s += s_red[w * V + k];
+    v[k] = s;
+  }
+  __syncthreads();
+}
+
+// ---------------------------------------------------------------- gather / init
+// adj: a = amp * (dL/dE, dL/dB) in tree order (SoA); rec16: the particle record
+// (x,y,z,gamma,ux,uy,uz,0) followed by (aE, aB, 0, 0) -- 128 bytes per particle.
+__global__ void adj_gather_kernel(int N, const uint32_t *__restrict__ perm, const double *__restrict__ ge,
+                                  const double *__restrict__ gb, double amp, const double *__restrict__ prec,
+                                  double *__restrict__ adj, double *__restrict__ rec16, double *__restrict__ gxu) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= N) return;
+  const int64_t o = 3 * (int64_t)perm[p];
+  double v[6];
+  for (int q = 0; q < 3; ++q) {
+    v[q] = amp * ge[o + q];
+    v[3 + q] = amp * gb[o + q];
+  }
+  double *r = rec16 + 16 * (int64_t)p;
+  for (int q = 0; q < 8; ++q) r[q] = prec[8 * (int64_t)p + q];
+  for (int q = 0; q < 6; ++q) {
+    adj[(int64_t)q * N + p] = v[q];
+    r[8 + q] = v[q];
+    gxu[(int64_t)q * N + p] = 0.0;
+  }
+  r[14] = 0.0;
+  r[15] = 0.0;
+}
+
+// ---------------------------------------------------------------- L2P^T / P2M^T (per leaf)
+// MODE 0 (L2P^T): fields F = leaf locals (6), adjoint a_p (6): gx_p += sum_q a_q dF_q/dx;
+//   also gloc[leaf] += sum_p a_p w(x_p).
+// MODE 1 (P2M^T): fields F = leaf moment adjoints (4): gu_p += I_M + I_G u/gamma,
+//   gx_p += gamma dI_G/dx + u . dI_M/dx.
+constexpr int kBwdChunk = 64;
+
+template <int NDEG, int MODE>
+__global__ void __launch_bounds__(128)
+    leaf_bwd_kernel(int leaf0, const int *__restrict__ lohi, const double *__restrict__ nodes,
+                    const double *__restrict__ bbox, const double *__restrict__ prec,
+                    const double *__restrict__ field, const double *__restrict__ adj, int N,
+                    double *__restrict__ gxu, double *__restrict__ gloc, double *__restrict__ gbox) {
+  using S = BShape<NDEG>;
+  constexpr int M = S::M, NN = S::NN, NS = S::NS;
+  constexpr int Q = MODE == 0 ? 6 : 4;
+  extern __shared__ __align__(16) unsigned char smem[];
+  double *s_f = (double *)smem;  // Q*NN
+  __shared__ double s_n[3 * M];
+  __shared__ double s_red[32 * 6];
+  __shared__ double s_w[kBwdChunk][3][M];
+  __shared__ double s_a[kBwdChunk][6];
+  const int tid = threadIdx.x;
+  const int c = leaf0 + blockIdx.x;
+  const int lo = lohi[2 * c], hi = lohi[2 * c + 1];
+  const double *bb = bbox + 6 * (int64_t)c;
+  const double *fc = field + (int64_t)c * Q * NN;
+  for (int e = tid; e < Q * NN; e += blockDim.x) s_f[e] = fc[e];
+  for (int i = tid; i < 3 * M; i += blockDim.x) s_n[i] = nodes[(int64_t)c * NS + i];
+  __syncthreads();
+  double gbx[6] = {0, 0, 0, 0, 0, 0};
+  for (int p = lo + tid; p <= hi; p += blockDim.x) {
+    const double *r = prec + 8 * (int64_t)p;
+    double w[3][M], dw[3][M];
+    weights_d64<M>(r[0], s_n, w[0], dw[0]);
+    weights_d64<M>(r[1], s_n + M, w[1], dw[1]);
+    weights_d64<M>(r[2], s_n + 2 * M, w[2], dw[2]);
+    double I[Q], D[3][Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      const double *F = s_f + q * NN;
+      double vi = 0, dx = 0, dy = 0, dz = 0;
+      for (int k = 0; k < M; ++k) {
+        double ay = 0, ady = 0, axd = 0;
+#pragma unroll
+        for (int j = 0; j < M; ++j) {
+          const double *row = F + M * (j + M * k);
+          double vx = 0, vdx = 0;
+#pragma unroll
+          for (int i = 0; i < M; ++i) {
+            vx += w[0][i] * row[i];
+            vdx += dw[0][i] * row[i];
+          }
+          ay += w[1][j] * vx;
+          ady += dw[1][j] * vx;
+          axd += w[1][j] * vdx;
+        }
+        vi += w[2][k] * ay;
+        dx += w[2][k] * axd;
+        dy += w[2][k] * ady;
+        dz += dw[2][k] * ay;
+      }
+      I[q] = vi;
+      D[0][q] = dx;
+      D[1][q] = dy;
+      D[2][q] = dz;
+    }
+    double G[3];
+    if (MODE == 0) {
+      double a[6];
+#pragma unroll
+      for (int q = 0; q < 6; ++q) a[q] = adj[(int64_t)q * N + p];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        double g = 0;
+#pragma unroll
+        for (int q = 0; q < 6; ++q) g += a[q] * D[d][q];
+        G[d] = g;
+      }
+    } else {
+      const double gam = r[3], ux = r[4], uy = r[5], uz = r[6];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) G[d] = gam * D[d][0] + ux * D[d][1] + uy * D[d][2] + uz * D[d][3];
+      const double ig = I[0] / gam;
+      gxu[(int64_t)3 * N + p] += I[1] + ig * ux;
+      gxu[(int64_t)4 * N + p] += I[2] + ig * uy;
+      gxu[(int64_t)5 * N + p] += I[3] + ig * uz;
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      gxu[(int64_t)d * N + p] += G[d];
+      const double a = bb[d], b = bb[3 + d], wd = b - a;
+      if (wd > 0.0) {
+        const double xi = (r[d] - a) / wd;
+        gbx[d] += (xi - 1.0) * G[d];
+        gbx[3 + d] += -xi * G[d];
+      }
+    }
+  }
+  block_sum<6>(gbx, s_red);
+  if (tid < 6) gbox[6 * (int64_t)c + tid] += gbx[tid];
+  if (MODE == 0) {
+    // gloc[leaf][q][a] += sum_p a_p[q] w_a(x_p)
+    double acc[(NN + 127) / 128][6];
+#pragma unroll
+    for (int r = 0; r < (NN + 127) / 128; ++r)
+#pragma unroll
+      for (int q = 0; q < 6; ++q) acc[r][q] = 0.0;
+    for (int c0 = lo; c0 <= hi; c0 += kBwdChunk) {
+      const int cnt = (hi - c0 + 1) < kBwdChunk ? (hi - c0 + 1) : kBwdChunk;
+      __syncthreads();
+      for (int task = tid; task < 3 * cnt; task += blockDim.x) {
+        const int p = task / 3, d = task % 3;
+        weights64<M>(prec[8 * (int64_t)(c0 + p) + d], s_n + d * M, s_w[p][d]);
+      }
+      for (int task = tid; task < 6 * cnt; task += blockDim.x) {
+        const int p = task / 6, q = task % 6;
+        s_a[p][q] = adj[(int64_t)q * N + c0 + p];
+      }
+      __syncthreads();
+#pragma unroll
+      for (int r = 0; r < (NN + 127) / 128; ++r) {
+        const int a = tid + 128 * r;
+        if (a < NN) {
+          const int ai = a % M, aj = (a / M) % M, ak = a / (M * M);
+          for (int p = 0; p < cnt; ++p) {
+            const double wt = s_w[p][0][ai] * s_w[p][1][aj] * s_w[p][2][ak];
+#pragma unroll
+            for (int q = 0; q < 6; ++q) acc[r][q] += s_a[p][q] * wt;
+          }
+        }
+      }
+    }
+    double *gl = gloc + (int64_t)c * 6 * NN;
+#pragma unroll
+    for (int r = 0; r < (NN + 127) / 128; ++r) {
+      const int a = tid + 128 * r;
+      if (a < NN)
+#pragma unroll
+        for (int q = 0; q < 6; ++q) gl[q * NN + a] += acc[r][q];
+    }
+  }
+}
+
+// ---------------------------------------------------------------- L2L^T / M2M^T (per parent)
+// The transfer T_c: child[i] = sum_I parent[I] W_c[i][I], W_c = Lx (x) Ly (x) Lz with
+// L[d][i][I] = w_I^{parent}(x^{child}_{d,i}).
+// MODE 0 (L2L^T, children at clevel): gP += T_c^T gC over both children; geometry with
+//   X_c = gC (child local adjoint), Y_P = the parent's final locals.
+// MODE 1 (M2M^T, parents at plevel): gC += T_c gP; geometry with X_c = the child's
+//   moments, Y_P = gP (the parent's moment adjoint).
+// Geometry: G_d[i] = sum_q sum_{(i,j,k): i_d = i} X_c[q][ijk] (T_c^{(d)} Y_P)[q][ijk] where
+// T^{(d)} uses the derivative weights on axis d.
+template <int NDEG, int MODE>
+__global__ void __launch_bounds__(BShape<NDEG>::BT)
+    transfer_bwd_kernel(int plevel, const double *__restrict__ nodes, const double *__restrict__ bbox, ChebT ct,
+                        const double *__restrict__ Xfield, const double *__restrict__ Yfield,
+                        double *__restrict__ gfield, double *__restrict__ gbox) {
+  using S = BShape<NDEG>;
+  constexpr int M = S::M, NN = S::NN, NS = S::NS, BT = S::BT, NPT = S::NPT;
+  constexpr int Q = MODE == 0 ? 6 : 4;
+  extern __shared__ __align__(16) unsigned char smem[];
+  double *s_x = (double *)smem;  // NN
+  double *s_y = s_x + NN;        // NN
+  double *s_t1 = s_y + NN;       // NN
+  double *s_t2 = s_t1 + NN;      // NN
+  double *s_e = s_t2 + NN;       // 3*NN products for the three axes
+  __shared__ double L[2][3][M][M], D[2][3][M][M];
+  __shared__ double s_G[2][3][M];
+  const int tid = threadIdx.x;
+  const int p = (1 << plevel) - 1 + blockIdx.x;
+  const int c1 = 2 * p + 1;
+  for (int task = tid; task < 2 * 3 * M; task += BT) {
+    const int ch = task / (3 * M), r = task % (3 * M), d = r / M, i = r % M;
+    const double x = nodes[(int64_t)(c1 + ch) * NS + d * M + i];
+    weights_d64<M>(x, nodes + (int64_t)p * NS + d * M, L[ch][d][i], D[ch][d][i]);
+  }
+  double accP[NPT][Q];  // MODE 0: parent adjoint accumulation
+#pragma unroll
+  for (int r = 0; r < NPT; ++r)
+#pragma unroll
+    for (int q = 0; q < Q; ++q) accP[r][q] = 0.0;
+  for (int e = tid; e < 2 * 3 * M; e += BT) (&s_G[0][0][0])[e] = 0.0;
+  __syncthreads();
+
+  for (int ch = 0; ch < 2; ++ch) {
+    const int c = c1 + ch;
+    double eacc[NPT][3];
+#pragma unroll
+    for (int r = 0; r < NPT; ++r) eacc[r][0] = eacc[r][1] = eacc[r][2] = 0.0;
+    for (int q = 0; q < Q; ++q) {
+      const double *X = (MODE == 0 ? Xfield + (int64_t)c * Q * NN : Xfield + (int64_t)c * Q * NN) + q * NN;
+      const double *Y = (MODE == 0 ? Yfield + (int64_t)p * Q * NN : Yfield + (int64_t)p * Q * NN) + q * NN;
+      for (int e = tid; e < NN; e += BT) {
+        s_x[e] = X[e];
+        s_y[e] = Y[e];
+      }
+      __syncthreads();
+      // adjoint propagation
+      if (MODE == 0) {
+        // parent[I] += sum_i W[i][I] gC[i] (contract x, y, z over the child index)
+        for (int e = tid; e < NN; e += BT) {
+          const int I = e % M, jk = e / M;
+          double v = 0;
+#pragma unroll
+          for (int i = 0; i < M; ++i) v += L[ch][0][i][I] * s_x[i + M * jk];
+          s_t1[e] = v;
+        }
+        __syncthreads();
+        for (int e = tid; e < NN; e += BT) {
+          const int I = e % M, J = (e / M) % M, k = e / (M * M);
+          double v = 0;
+#pragma unroll
+          for (int j = 0; j < M; ++j) v += L[ch][1][j][J] * s_t1[I + M * j + M * M * k];
+          s_t2[e] = v;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < NPT; ++r) {
+          const int a = tid + r * BT;
+          if (a < NN) {
+            const int IJ = a % (M * M), K = a / (M * M);
+            double v = 0;
+#pragma unroll
+            for (int k = 0; k < M; ++k) v += L[ch][2][k][K] * s_t2[IJ + M * M * k];
+            accP[r][q] += v;
+          }
+        }
+        __syncthreads();
+      } else {
+        // child[i] += sum_I W[i][I] gP[I]
+        for (int e = tid; e < NN; e += BT) {
+          const int i = e % M, JK = e / M;
+          double v = 0;
+#pragma unroll
+          for (int I = 0; I < M; ++I) v += L[ch][0][i][I] * s_y[I + M * JK];
+          s_t1[e] = v;
+        }
+        __syncthreads();
+        for (int e = tid; e < NN; e += BT) {
+          const int i = e % M, j = (e / M) % M, K = e / (M * M);
+          double v = 0;
+#pragma unroll
+          for (int J = 0; J < M; ++J) v += L[ch][1][j][J] * s_t1[i + M * J + M * M * K];
+          s_t2[e] = v;
+        }
+        __syncthreads();
+        double *gc = gfield + (int64_t)c * Q * NN + q * NN;
+        for (int e = tid; e < NN; e += BT) {
+          const int ij = e % (M * M), k = e / (M * M);
+          double v = 0;
+#pragma unroll
+          for (int K = 0; K < M; ++K) v += L[ch][2][k][K] * s_t2[ij + M * M * K];
+          gc[e] += v;
+        }
+        __syncthreads();
+      }
+      // geometry: e_d[a] += X[a] * (T^{(d)} Y)[a] for d = x, y, z
+      for (int d = 0; d < 3; ++d) {
+        const double(*Wx)[M] = d == 0 ? D[ch][0] : L[ch][0];
+        const double(*Wy)[M] = d == 1 ? D[ch][1] : L[ch][1];
+        const double(*Wz)[M] = d == 2 ? D[ch][2] : L[ch][2];
+        for (int e = tid; e < NN; e += BT) {
+          const int i = e % M, JK = e / M;
+          double v = 0;
+#pragma unroll
+          for (int I = 0; I < M; ++I) v += Wx[i][I] * s_y[I + M * JK];
+          s_t1[e] = v;
+        }
+        __syncthreads();
+        for (int e = tid; e < NN; e += BT) {
+          const int i = e % M, j = (e / M) % M, K = e / (M * M);
+          double v = 0;
+#pragma unroll
+          for (int J = 0; J < M; ++J) v += Wy[j][J] * s_t1[i + M * J + M * M * K];
+          s_t2[e] = v;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < NPT; ++r) {
+          const int a = tid + r * BT;
+          if (a < NN) {
+            const int ij = a % (M * M), k = a / (M * M);
+            double v = 0;
+#pragma unroll
+            for (int K = 0; K < M; ++K) v += Wz[k][K] * s_t2[ij + M * M * K];
+            eacc[r][d] += s_x[a] * v;
+          }
+        }
+        __syncthreads();
+      }
+    }
+    // G_d[i] = sum over the nodes with index i on axis d
+#pragma unroll
+    for (int r = 0; r < NPT; ++r) {
+      const int a = tid + r * BT;
+      if (a < NN) {
+        s_e[a] = eacc[r][0];
+        s_e[NN + a] = eacc[r][1];
+        s_e[2 * NN + a] = eacc[r][2];
+      }
+    }
+    __syncthreads();
+    if (tid < 3 * M) {
+      const int d = tid / M, i = tid % M;
+      double g = 0;
+      for (int u = 0; u < M; ++u)
+        for (int v = 0; v < M; ++v) {
+          const int a = d == 0 ? i + M * (u + M * v) : (d == 1 ? u + M * (i + M * v) : u + M * (v + M * i));
+          g += s_e[d * NN + a];
+        }
+      s_G[ch][d][i] = g;
+    }
+    __syncthreads();
+  }
+  // boxes: the child's nodes move with its box; the parent's weights with the parent's box
+  if (tid < 6 * 3) {
+    const int who = tid / 6, k = tid % 6, d = k % 3, side = k / 3;  // who: 0,1 children, 2 parent
+    double g = 0;
+    if (who < 2) {
+      for (int i = 0; i < M; ++i) g += (side == 0 ? 1.0 - ct.t[i] : ct.t[i]) * s_G[who][d][i];
+      gbox[6 * (int64_t)(c1 + who) + k] += g;
+    } else {
+      const double a = bbox[6 * (int64_t)p + d], b = bbox[6 * (int64_t)p + 3 + d], wd = b - a;
+      if (wd > 0.0)
+        for (int ch = 0; ch < 2; ++ch)
+          for (int i = 0; i < M; ++i) {
+            const double xi = (nodes[(int64_t)(c1 + ch) * NS + d * M + i] - a) / wd;
+            g += (side == 0 ? xi - 1.0 : -xi) * s_G[ch][d][i];
+          }
+      gbox[6 * (int64_t)p + k] += g;
+    }
+  }
+  if (MODE == 0) {
+    double *gp = gfield + (int64_t)p * Q * NN;
+#pragma unroll
+    for (int r = 0; r < NPT; ++r) {
+      const int a = tid + r * BT;
+      if (a < NN)
+#pragma unroll
+        for (int q = 0; q < Q; ++q) gp[q * NN + a] += accP[r][q];
+    }
+  }
+}
+
+// ---------------------------------------------------------------- M2L^T (per target cluster)
+// Over the union U(t) of {s : (t,s) in list} (flag 1) and {s : (s,t) in list}
+// (flag 2), with R = x_a - x_b, f = d^{-3/2}, K = f R:
+//   c1 = Gamma_s[b] gE_t[a] + gB_t[a] x M_s[b]      (t is the target)
+//   c2 = Gamma_t[a] gE_s[b] + gB_s[b] x M_t[a]      (t is the source)
+//   gx_a     += f c - 3 d^{-5/2} (R.c)(R + (p.R) p),  c = [f1] c1 - [f2] c2
+//   gGamma_a -= [f2] f gE_s[b].R,   gM_a -= [f2] f R x gB_s[b]
+//   gp       += [f1] -3 d^{-5/2} (p.R)(R.c1) R
+template <int NDEG>
+__global__ void __launch_bounds__(BShape<NDEG>::BT)
+    m2l_bwd_kernel(const int *__restrict__ ptr, const int *__restrict__ src, const uint8_t *__restrict__ flg,
+                   const double *__restrict__ nodes, ChebT ct, const double *__restrict__ mom,
+                   const double *__restrict__ gloc, const double *__restrict__ consts, double *__restrict__ gmom,
+                   double *__restrict__ gbox, double *__restrict__ gp_part, int *__restrict__ status) {
+  using S = BShape<NDEG>;
+  constexpr int M = S::M, NN = S::NN, NS = S::NS, BT = S::BT, NPT = S::NPT;
+  constexpr int REC = 10 * NN + NS;  // Gamma, M(3), gE(3), gB(3) | nodes
+  extern __shared__ __align__(16) unsigned char smem[];
+  double *buf = (double *)smem;  // 2 * REC
+  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ double s_red[32 * 6];
+  const int tid = threadIdx.x;
+  const int t = blockIdx.x;
+  const int p0 = ptr[t], np = ptr[t + 1] - p0;
+  const double *tn = nodes + (int64_t)t * NS;
+  const double px = consts[0], py = consts[1], pz = consts[2];
+  double gx[NPT][3], gG[NPT], gM[NPT][3], gp[3] = {0, 0, 0};
+  double own[NPT][10];  // Gamma_a, M_a(3), gE_a(3), gB_a(3)
+#pragma unroll
+  for (int r = 0; r < NPT; ++r) {
+    gx[r][0] = gx[r][1] = gx[r][2] = gG[r] = gM[r][0] = gM[r][1] = gM[r][2] = 0.0;
+    const int a = tid + r * BT;
+#pragma unroll
+    for (int q = 0; q < 10; ++q) own[r][q] = 0.0;
+    if (a < NN) {
+      const double *ma = mom + (int64_t)t * 4 * NN, *la = gloc + (int64_t)t * 6 * NN;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) own[r][q] = ma[q * NN + a];
+#pragma unroll
+      for (int q = 0; q < 6; ++q) own[r][4 + q] = la[q * NN + a];
+    }
+  }
+  if (np > 0) {
+    if (tid == 0) {
+      mbar_init(&bar[0], 1);
+      mbar_init(&bar[1], 1);
+      fence_mbar_init();
+    }
+    __syncthreads();
+    auto issue = [&](int k, int bb) {
+      const int s = src[p0 + k];
+      double *dst = buf + bb * REC;
+      mbar_arrive_expect_tx(&bar[bb], REC * 8);
+      bulk_g2s(dst, mom + (int64_t)s * 4 * NN, 4 * NN * 8, &bar[bb]);
+      bulk_g2s(dst + 4 * NN, gloc + (int64_t)s * 6 * NN, 6 * NN * 8, &bar[bb]);
+      bulk_g2s(dst + 10 * NN, nodes + (int64_t)s * NS, NS * 8, &bar[bb]);
+    };
+    if (tid == 0) issue(0, 0);
+    for (int it = 0; it < np; ++it) {
+      const int bb = it & 1;
+      const int fl = flg[p0 + it];
+      if (tid == 0 && it + 1 < np) {
+        fence_proxy_async_smem();
+        issue(it + 1, bb ^ 1);
+      }
+      const bool ok = mbar_wait_bounded(&bar[bb], (uint32_t)((it >> 1) & 1), status);
+      if (ok) {
+        const double *B = buf + bb * REC;
+        const double *SN = B + 10 * NN;
+        const bool f1 = fl & 1, f2 = fl & 2;
+#pragma unroll
+        for (int r = 0; r < NPT; ++r) {
+          const int a = tid + r * BT;
+          if (a >= NN) continue;
+          const int ai = a % M, aj = (a / M) % M, ak = a / (M * M);
+          const double tx = tn[ai], ty = tn[M + aj], tz = tn[2 * M + ak];
+          const double Ga = own[r][0], Ma0 = own[r][1], Ma1 = own[r][2], Ma2 = own[r][3];
+          const double gEa0 = own[r][4], gEa1 = own[r][5], gEa2 = own[r][6];
+          const double gBa0 = own[r][7], gBa1 = own[r][8], gBa2 = own[r][9];
+          double rxv[M], prx[M], rx2[M];
+#pragma unroll
+          for (int bi = 0; bi < M; ++bi) {
+            rxv[bi] = tx - SN[bi];
+            prx[bi] = px * rxv[bi];
+            rx2[bi] = rxv[bi] * rxv[bi];
+          }
+          double ax0 = 0, ax1 = 0, ax2 = 0, aG = 0, aM0 = 0, aM1 = 0, aM2 = 0, ap0 = 0, ap1 = 0, ap2 = 0;
+#pragma unroll 1
+          for (int bk = 0; bk < M; ++bk) {
+            const double rz = tz - SN[2 * M + bk];
+            const double prz = pz * rz, rz2 = rz * rz + kEps64;
+            for (int bj = 0; bj < M; ++bj) {
+              const double ry = ty - SN[M + bj];
+              const double P = py * ry + prz, A = ry * ry + rz2;
+              const int b0 = M * (bj + M * bk);
+#pragma unroll
+              for (int bi = 0; bi < M; ++bi) {
+                const int b = b0 + bi;
+                const double rx = rxv[bi];
+                const double pr = P + prx[bi];
+                const double d = pr * pr + (A + rx2[bi]);
+                const double s = rsqrt(d);
+                const double f = s * s * s, f5 = f * s * s;
+                double c0 = 0, c1 = 0, c2 = 0;
+                if (f1) {
+                  const double gs = B[b], m0 = B[NN + b], m1 = B[2 * NN + b], m2 = B[3 * NN + b];
+                  c0 = gs * gEa0 + (gBa1 * m2 - gBa2 * m1);
+                  c1 = gs * gEa1 + (gBa2 * m0 - gBa0 * m2);
+                  c2 = gs * gEa2 + (gBa0 * m1 - gBa1 * m0);
+                  const double w = -3.0 * f5 * pr * (rx * c0 + ry * c1 + rz * c2);
+                  ap0 += w * rx;
+                  ap1 += w * ry;
+                  ap2 += w * rz;
+                }
+                if (f2) {
+                  const double e0 = B[4 * NN + b], e1 = B[5 * NN + b], e2 = B[6 * NN + b];
+                  const double h0 = B[7 * NN + b], h1 = B[8 * NN + b], h2 = B[9 * NN + b];
+                  c0 -= Ga * e0 + (h1 * Ma2 - h2 * Ma1);
+                  c1 -= Ga * e1 + (h2 * Ma0 - h0 * Ma2);
+                  c2 -= Ga * e2 + (h0 * Ma1 - h1 * Ma0);
+                  aG -= f * (e0 * rx + e1 * ry + e2 * rz);
+                  aM0 -= f * (ry * h2 - rz * h1);
+                  aM1 -= f * (rz * h0 - rx * h2);
+                  aM2 -= f * (rx * h1 - ry * h0);
+                }
+                const double w3 = 3.0 * f5 * (rx * c0 + ry * c1 + rz * c2);
+                ax0 += f * c0 - w3 * (rx + pr * px);
+                ax1 += f * c1 - w3 * (ry + pr * py);
+                ax2 += f * c2 - w3 * (rz + pr * pz);
+              }
+            }
+          }
+          gx[r][0] += ax0;
+          gx[r][1] += ax1;
+          gx[r][2] += ax2;
+          gG[r] += aG;
+          gM[r][0] += aM0;
+          gM[r][1] += aM1;
+          gM[r][2] += aM2;
+          gp[0] += ap0;
+          gp[1] += ap1;
+          gp[2] += ap2;
+        }
+      }
+      __syncthreads();
+    }
+  }
+  // moment adjoints (source role) and the target box from the node-position gradients
+  double gbx[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll
+  for (int r = 0; r < NPT; ++r) {
+    const int a = tid + r * BT;
+    if (a >= NN) continue;
+    double *gm = gmom + (int64_t)t * 4 * NN;
+    gm[a] += gG[r];
+    gm[NN + a] += gM[r][0];
+    gm[2 * NN + a] += gM[r][1];
+    gm[3 * NN + a] += gM[r][2];
+    const int idx[3] = {a % M, (a / M) % M, a / (M * M)};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      gbx[d] += (1.0 - ct.t[idx[d]]) * gx[r][d];
+      gbx[3 + d] += ct.t[idx[d]] * gx[r][d];
+    }
+  }
+  block_sum<6>(gbx, s_red);
+  if (tid < 6) gbox[6 * (int64_t)t + tid] += gbx[tid];
+  double g3[6] = {gp[0], gp[1], gp[2], 0, 0, 0};
+  block_sum<6>(g3, s_red);
+  if (tid < 3) gp_part[3 * (int64_t)t + tid] = g3[tid];
+}
+
+// ---------------------------------------------------------------- P2P^T (per target leaf)
+// Per target particle p over the particles j of every source leaf in the union list:
+//   (t <- s), flag 1: K1 = K(R; u_j), c1 = gamma_j a_E,p + a_B,p x u_j:
+//        gx_p += J1^T c1 = f1 c1 - 3 d1^{-5/2} (R.c1)(R + (u_j.R) u_j)
+//   (s <- t), flag 2: K2 = K(-R; u_p), c2 = gamma_p a_E,j + a_B,j x u_p:
+//        gx_p -= J2^T c2;  gu_p += 3 d2^{-5/2}(R.c2)(u_p.R) R - f2 (a_E,j.R) u_p/gamma_p - f2 R x a_B,j
+// with R = x_p - x_j; the self pair j = p is skipped.
+constexpr int kPbTile = 64;
+
+template <int G>
+__global__ void __launch_bounds__(128)
+    p2p_bwd_kernel(int leaf0, const int *__restrict__ lohi, const int *__restrict__ ptr, const int *__restrict__ src,
+                   const uint8_t *__restrict__ flg, const double *__restrict__ rec16, int N,
+                   double *__restrict__ gxu, int *__restrict__ status) {
+  __shared__ __align__(16) double buf[2][kPbTile * 16];
+  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ int meta[2][3];  // cnt, flag, first tree index
+  __shared__ int s_warp[33];
+  const int tid = threadIdx.x, TP = blockDim.x / G, tl = tid / G, g = tid % G;
+  const int c = leaf0 + blockIdx.x;
+  const int tlo = lohi[2 * c], thi = lohi[2 * c + 1], tcnt = thi - tlo + 1;
+  const int p0 = ptr[c], np = ptr[c + 1] - p0;
+  int w = 0;
+  for (int k = tid; k < np; k += blockDim.x) {
+    const int s = src[p0 + k];
+    w += (lohi[2 * s + 1] - lohi[2 * s] + kPbTile) / kPbTile;
+  }
+  int W;
+  block_excl_scan(w, s_warp, &W);
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  int wk = 0, woff = 0;
+  auto issue = [&](int bb) {
+    const int s = src[p0 + wk];
+    const int slo = lohi[2 * s], scnt = lohi[2 * s + 1] - slo + 1;
+    const int cnt = scnt - woff < kPbTile ? scnt - woff : kPbTile;
+    meta[bb][0] = cnt;
+    meta[bb][1] = flg[p0 + wk];
+    meta[bb][2] = slo + woff;
+    mbar_arrive_expect_tx(&bar[bb], (uint32_t)(cnt * 128));
+    bulk_g2s(&buf[bb][0], rec16 + 16 * (int64_t)(slo + woff), (uint32_t)(cnt * 128), &bar[bb]);
+    woff += kPbTile;
+    if (woff >= scnt) {
+      woff = 0;
+      ++wk;
+    }
+  };
+  int it = 0;
+  for (int tc = 0; tc < tcnt; tc += TP) {
+    const int ti = tc + tl;
+    const bool active = ti < tcnt;
+    const int pi = tlo + (active ? ti : 0);
+    const double *rp = rec16 + 16 * (int64_t)pi;
+    const double xp = rp[0], yp = rp[1], zp = rp[2], gp_ = rp[3], up0 = rp[4], up1 = rp[5], up2 = rp[6];
+    const double aE0 = rp[8], aE1 = rp[9], aE2 = rp[10], aB0 = rp[11], aB1 = rp[12], aB2 = rp[13];
+    double acc[6] = {0, 0, 0, 0, 0, 0};  // gx(3), gu(3)
+    if (tid == 0) {
+      wk = 0;
+      woff = 0;
+      if (W > 0) {
+        fence_proxy_async_smem();
+        issue(it & 1);
+      }
+    }
+    for (int i = 0; i < W; ++i, ++it) {
+      const int bb = it & 1;
+      if (tid == 0 && i + 1 < W) {
+        fence_proxy_async_smem();
+        issue(bb ^ 1);
+      }
+      const bool ok = mbar_wait_bounded(&bar[bb], (uint32_t)((it >> 1) & 1), status);
+      if (ok && active) {
+        const int cnt = meta[bb][0], fl = meta[bb][1], first = meta[bb][2];
+        for (int j = g; j < cnt; j += G) {
+          if (first + j == pi) continue;
+          const double *r = &buf[bb][16 * j];
+          const double rx = xp - r[0], ry = yp - r[1], rz = zp - r[2];
+          const double rr = rx * rx + ry * ry + rz * rz;
+          if (fl & 1) {
+            const double gj = r[3], u0 = r[4], u1 = r[5], u2 = r[6];
+            const double ur = u0 * rx + u1 * ry + u2 * rz;
+            const double s = rsqrt(rr + ur * ur + kEps64);
+            const double f = s * s * s, f5 = f * s * s;
+            const double k0 = gj * aE0 + (aB1 * u2 - aB2 * u1);
+            const double k1 = gj * aE1 + (aB2 * u0 - aB0 * u2);
+            const double k2 = gj * aE2 + (aB0 * u1 - aB1 * u0);
+            const double w3 = 3.0 * f5 * (rx * k0 + ry * k1 + rz * k2);
+            acc[0] += f * k0 - w3 * (rx + ur * u0);
+            acc[1] += f * k1 - w3 * (ry + ur * u1);
+            acc[2] += f * k2 - w3 * (rz + ur * u2);
+          }
+          if (fl & 2) {
+            const double e0 = r[8], e1 = r[9], e2 = r[10], h0 = r[11], h1 = r[12], h2 = r[13];
+            const double ur = up0 * rx + up1 * ry + up2 * rz;
+            const double s = rsqrt(rr + ur * ur + kEps64);
+            const double f = s * s * s, f5 = f * s * s;
+            const double k0 = gp_ * e0 + (h1 * up2 - h2 * up1);
+            const double k1 = gp_ * e1 + (h2 * up0 - h0 * up2);
+            const double k2 = gp_ * e2 + (h0 * up1 - h1 * up0);
+            const double w3 = 3.0 * f5 * (rx * k0 + ry * k1 + rz * k2);
+            acc[0] -= f * k0 - w3 * (rx + ur * up0);
+            acc[1] -= f * k1 - w3 * (ry + ur * up1);
+            acc[2] -= f * k2 - w3 * (rz + ur * up2);
+            const double er = (e0 * rx + e1 * ry + e2 * rz) * f / gp_;
+            const double wu = w3 * ur;
+            acc[3] += wu * rx - er * up0 - f * (ry * h2 - rz * h1);
+            acc[4] += wu * ry - er * up1 - f * (rz * h0 - rx * h2);
+            acc[5] += wu * rz - er * up2 - f * (rx * h1 - ry * h0);
+          }
+        }
+      }
+      __syncthreads();
+    }
+#pragma unroll
+    for (int q = 0; q < 6; ++q)
+#pragma unroll
+      for (int o = 1; o < G; o <<= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
+    if (active && g == 0)
+#pragma unroll
+      for (int q = 0; q < 6; ++q) gxu[(int64_t)q * N + pi] += acc[q];
+  }
+}
+
+// ---------------------------------------------------------------- boxes, p_avg, scatter
+// A box side of cluster c is attained by argext[c]: pass its adjoint to the child
+// holding that particle (levels top-down).
+__global__ void box_down_kernel(int l, const int *__restrict__ argext, double *__restrict__ gbox) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (1 << l)) return;
+  const int c = (1 << l) - 1 + idx, c1 = 2 * c + 1;
+  for (int k = 0; k < 6; ++k) {
+    const int who = argext[6 * (int64_t)c1 + k] == argext[6 * (int64_t)c + k] ? c1 : c1 + 1;
+    gbox[6 * (int64_t)who + k] += gbox[6 * (int64_t)c + k];
+  }
+}
+
+__global__ void box_leaf_kernel(int leaf0, int nleaf, const int *__restrict__ argext, const int *__restrict__ invperm,
+                                const double *__restrict__ gbox, int N, double *__restrict__ gxu) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= nleaf) return;
+  const int c = leaf0 + l;
+  for (int k = 0; k < 6; ++k) {
+    const int d = k % 3;
+    const int pos = invperm[argext[6 * (int64_t)c + k]];
+    gxu[(int64_t)d * N + pos] += gbox[6 * (int64_t)c + k];
+  }
+}
+
+__global__ void invperm_kernel(int N, const uint32_t *__restrict__ perm, int *__restrict__ inv) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < N) inv[perm[p]] = p;
+}
+
+// deterministic sum of the per-target p_avg adjoints (single block)
+__global__ void pbar_reduce_kernel(int64_t nc, const double *__restrict__ part, double *__restrict__ out) {
+  __shared__ double s[3][1024];
+  double v[3] = {0, 0, 0};
+  for (int64_t c = threadIdx.x; c < nc; c += blockDim.x)
+    for (int k = 0; k < 3; ++k) v[k] += part[3 * c + k];
+  for (int k = 0; k < 3; ++k) s[k][threadIdx.x] = v[k];
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o)
+      for (int k = 0; k < 3; ++k) s[k][threadIdx.x] += s[k][threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x < 3) out[threadIdx.x] = s[threadIdx.x][0];
+}
+
+__global__ void grad_scatter_kernel(int N, const uint32_t *__restrict__ perm, const double *__restrict__ gxu,
+                                    const double *__restrict__ gpbar, int use_pbar, double *__restrict__ gx,
+                                    double *__restrict__ gu) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= N) return;
+  const int64_t o = 3 * (int64_t)perm[p];
+  for (int d = 0; d < 3; ++d) {
+    gx[o + d] = gxu[(int64_t)d * N + p];
+    gu[o + d] = gxu[(int64_t)(3 + d) * N + p] + (use_pbar ? gpbar[d] / (double)N : 0.0);
+  }
+}
+
+template <int NDEG>
+int run_backward_t(Ctx *ctx, const double *d_ge, const double *d_gb, double *d_gx, double *d_gu) {
+  using S = BShape<NDEG>;
+  constexpr int M = S::M, NN = S::NN, NS = S::NS;
+  const int N = (int)ctx->N, ml = ctx->ml;
+  const int64_t nc = ctx->nc, nleaf = ctx->nleaf;
+  double *adj, *rec16, *gxu, *gloc, *gmom, *gbox, *gpp, *gpbar;
+  int *invp;
+  FMM_TRY(ctx->ensure("bwd_adj", 6 * (int64_t)N, &adj));
+  FMM_TRY(ctx->ensure("bwd_rec16", 16 * (int64_t)N, &rec16));
+  FMM_TRY(ctx->ensure("bwd_gxu", 6 * (int64_t)N, &gxu));
+  FMM_TRY(ctx->ensure("bwd_gloc", 6 * NN * nc, &gloc));
+  FMM_TRY(ctx->ensure("bwd_gmom", 4 * NN * nc, &gmom));
+  FMM_TRY(ctx->ensure("bwd_gbox", 6 * nc, &gbox));
+  FMM_TRY(ctx->ensure("bwd_gp_part", 3 * nc, &gpp));
+  FMM_TRY(ctx->ensure("bwd_gpbar", 4, &gpbar));
+  FMM_TRY(ctx->ensure("bwd_invperm", N, &invp));
+  cudaStream_t st = ctx->stream;
+  FMM_CUDA_TRY(ctx, cudaMemsetAsync(gloc, 0, sizeof(double) * 6 * NN * nc, st));
+  FMM_CUDA_TRY(ctx, cudaMemsetAsync(gmom, 0, sizeof(double) * 4 * NN * nc, st));
+  FMM_CUDA_TRY(ctx, cudaMemsetAsync(gbox, 0, sizeof(double) * 6 * nc, st));
+  const uint32_t *perm = ctx->get<uint32_t>("perm");
+  const double amp = kRe * ctx->charge / ctx->lambda;
+  adj_gather_kernel<<<ceil_div(N, 256), 256, 0, st>>>(N, perm, d_ge, d_gb, amp, ctx->get<double>("prec64"), adj,
+                                                      rec16, gxu);
+  FMM_TRY(ctx->check_launch("adj_gather_kernel"));
+  ChebT ct;
+  for (int i = 0; i < kMaxNodes1D; ++i) ct.t[i] = 0.0;
+  for (int i = 0; i < M; ++i) ct.t[i] = (std::cos(M_PI * (double)i / (double)NDEG) + 1.0) / 2.0;
+  const int *lohi = ctx->get<int>("lohi");
+  const double *nodes = ctx->get<double>("nodes"), *bbox = ctx->get<double>("bbox");
+  const double *prec = ctx->get<double>("prec64");
+  const double *loc = ctx->get<double>("loc64"), *mom = ctx->get<double>("mom64");
+  // L2P^T
+  {
+    auto k = leaf_bwd_kernel<NDEG, 0>;
+    const int sm = 6 * NN * 8;
+    FMM_TRY(opt_in_smem(ctx, k, sm));
+    k<<<(unsigned)nleaf, 128, sm, st>>>((int)ctx->leaf0, lohi, nodes, bbox, prec, loc, adj, N, gxu, gloc, gbox);
+    FMM_TRY(ctx->check_launch("leaf_bwd_kernel<L2P>"));
+  }
+  // L2L^T, children at levels ml .. 1
+  {
+    auto k = transfer_bwd_kernel<NDEG, 0>;
+    const int sm = 7 * NN * 8;
+    FMM_TRY(opt_in_smem(ctx, k, sm));
+    for (int l = ml; l >= 1; --l) {
+      k<<<1u << (l - 1), S::BT, sm, st>>>(l - 1, nodes, bbox, ct, gloc, loc, gloc, gbox);
+      FMM_TRY(ctx->check_launch("transfer_bwd_kernel<L2L>"));
+    }
+  }
+  // M2L^T over the union lists
+  {
+    auto k = m2l_bwd_kernel<NDEG>;
+    const int sm = 2 * (10 * NN + NS) * 8;
+    FMM_TRY(opt_in_smem(ctx, k, sm));
+    k<<<(unsigned)nc, S::BT, sm, st>>>(ctx->get<int>("m2lu_ptr"), ctx->get<int>("m2lu_src"),
+                                        ctx->get<uint8_t>("m2lu_flag"), nodes, ct, mom, gloc, ctx->get<double>("consts"),
+                                        gmom, gbox, gpp, ctx->d_status);
+    FMM_TRY(ctx->check_launch("m2l_bwd_kernel"));
+  }
+  // M2M^T, parents at levels 0 .. ml-1 (top-down)
+  {
+    auto k = transfer_bwd_kernel<NDEG, 1>;
+    const int sm = 7 * NN * 8;
+    FMM_TRY(opt_in_smem(ctx, k, sm));
+    for (int l = 0; l < ml; ++l) {
+      k<<<1u << l, S::BT, sm, st>>>(l, nodes, bbox, ct, mom, gmom, gmom, gbox);
+      FMM_TRY(ctx->check_launch("transfer_bwd_kernel<M2M>"));
+    }
+  }
+  // P2M^T
+  {
+    auto k = leaf_bwd_kernel<NDEG, 1>;
+    const int sm = 4 * NN * 8;
+    FMM_TRY(opt_in_smem(ctx, k, sm));
+    k<<<(unsigned)nleaf, 128, sm, st>>>((int)ctx->leaf0, lohi, nodes, bbox, prec, gmom, adj, N, gxu, gloc, gbox);
+    FMM_TRY(ctx->check_launch("leaf_bwd_kernel<P2M>"));
+  }
+  // P2P^T (G lanes per target particle as in the forward)
+  {
+    const int *pp = ctx->get<int>("p2pu_ptr"), *ps = ctx->get<int>("p2pu_src");
+    const uint8_t *pf = ctx->get<uint8_t>("p2pu_flag");
+    if (ctx->max_leaf <= 32)
+      p2p_bwd_kernel<4><<<(unsigned)nleaf, 128, 0, st>>>((int)ctx->leaf0, lohi, pp, ps, pf, rec16, N, gxu, ctx->d_status);
+    else if (ctx->max_leaf <= 64)
+      p2p_bwd_kernel<2><<<(unsigned)nleaf, 128, 0, st>>>((int)ctx->leaf0, lohi, pp, ps, pf, rec16, N, gxu, ctx->d_status);
+    else
+      p2p_bwd_kernel<1><<<(unsigned)nleaf, 128, 0, st>>>((int)ctx->leaf0, lohi, pp, ps, pf, rec16, N, gxu, ctx->d_status);
+    FMM_TRY(ctx->check_launch("p2p_bwd_kernel"));
+  }
+  // boxes -> extremal particles; p_avg -> every momentum; scatter to caller order
+  const int *argext = ctx->get<int>("argext");
+  for (int l = 0; l < ml; ++l) {
+    box_down_kernel<<<ceil_div(1 << l, 256), 256, 0, st>>>(l, argext, gbox);
+    FMM_TRY(ctx->check_launch("box_down_kernel"));
+  }
+  invperm_kernel<<<ceil_div(N, 256), 256, 0, st>>>(N, perm, invp);
+  box_leaf_kernel<<<ceil_div(nleaf, 256), 256, 0, st>>>((int)ctx->leaf0, (int)nleaf, argext, invp, gbox, N, gxu);
+  pbar_reduce_kernel<<<1, 1024, 0, st>>>(nc, gpp, gpbar);
+  grad_scatter_kernel<<<ceil_div(N, 256), 256, 0, st>>>(N, perm, gxu, gpbar, ctx->pavg_from_momenta ? 1 : 0, d_gx,
+                                                        d_gu);
+  FMM_TRY(ctx->check_launch("box/pbar/scatter kernels", 4));
+  return FMMB200_OK;
+}
+
+}  // namespace
+
+int run_backward(Ctx *ctx, const double *d_ge, const double *d_gb, double *d_gx, double *d_gu) {
+  switch (ctx->n) {
+    case 1: return run_backward_t<1>(ctx, d_ge, d_gb, d_gx, d_gu);
+    case 2: return run_backward_t<2>(ctx, d_ge, d_gb, d_gx, d_gu);
+    case 3: return run_backward_t<3>(ctx, d_ge, d_gb, d_gx, d_gu);
+    case 4: return run_backward_t<4>(ctx, d_ge, d_gb, d_gx, d_gu);
+    case 5: return run_backward_t<5>(ctx, d_ge, d_gb, d_gx, d_gu);
+    case 6: return run_backward_t<6>(ctx, d_ge, d_gb, d_gx, d_gu);
+    case 7: return run_backward_t<7>(ctx, d_ge, d_gb, d_gx, d_gu);
+    case 8: return run_backward_t<8>(ctx, d_ge, d_gb, d_gx, d_gu);
+    default:
+      return ctx->fail(FMMB200_ERR_INVALID_ARGUMENT, "the adjoint supports degrees n = 1..8");
+  }
+}
+
+}  // namespace fmmb200

@@ -35,6 +35,7 @@ struct fmmb200_ctx {
   bool have_lists = false;   // interaction lists valid
   bool have_forward = false; // expansions of a forward valid
   bool saved = false;        // forward saved for backward
+  bool pavg_from_momenta = true;  // p_avg = sum(u)/N was computed here (so it depends on u)
   int64_t N = 0, N0 = 0;
   int n = 0, precision = 0;
   int ml = 0;

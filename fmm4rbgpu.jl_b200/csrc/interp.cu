@@ -16,6 +16,7 @@
 // the P2P near field, the amp normalisation and the scatter back to the
 // caller's particle order.
 #include "device_util.cuh"
+#include "interp_util.cuh"
 #include "kernels.cuh"
 
 namespace fmmb200 {
@@ -30,58 +31,6 @@ struct Grid {
   static constexpr int BT = NN <= 64 ? 64 : (NN <= 512 ? ((NN + 31) / 32) * 32 : 512);
   static constexpr int NPT = (NN + BT - 1) / BT;
 };
-
-// second-kind barycentric weights: 1/2, -1, 1, ..., (-1)^n/2
-__device__ __forceinline__ double bary_ws(int i, int M) {
-  double w = (i & 1) ? -1.0 : 1.0;
-  return (i == 0 || i == M - 1) ? 0.5 * w : w;
-}
-
-// FP64 weights of the M nodes at x (GPU exact-node semantics).
-template <int M, typename TW>
-__device__ __forceinline__ void weights64(double x, const double *nodes, TW *w) {
-  double q[M];
-  double sum = 0.0;
-  int flag = -1;
-#pragma unroll
-  for (int i = 0; i < M; ++i) {
-    const double dx = x - nodes[i];
-    flag = fabs(dx) < kEps64 ? i : flag;
-    q[i] = bary_ws(i, M) / dx;
-    sum += q[i];
-  }
-  if (flag >= 0) {
-#pragma unroll
-    for (int i = 0; i < M; ++i) w[i] = (TW)(i == flag ? 1.0 : 0.0);
-  } else {
-    const double inv = 1.0 / sum;
-#pragma unroll
-    for (int i = 0; i < M; ++i) w[i] = (TW)(q[i] * inv);
-  }
-}
-
-// FP32 weights from leaf-local FP32 coordinates (exact hit: dx == 0 or subnormal).
-template <int M>
-__device__ __forceinline__ void weights32(float x, const float *nodes, float *w) {
-  float q[M];
-  float sum = 0.f;
-  int flag = -1;
-#pragma unroll
-  for (int i = 0; i < M; ++i) {
-    const float dx = x - nodes[i];
-    flag = fabsf(dx) < 1.17549435e-38f ? i : flag;
-    q[i] = (float)bary_ws(i, M) / dx;
-    sum += q[i];
-  }
-  if (flag >= 0) {
-#pragma unroll
-    for (int i = 0; i < M; ++i) w[i] = i == flag ? 1.f : 0.f;
-  } else {
-    const float inv = 1.f / sum;
-#pragma unroll
-    for (int i = 0; i < M; ++i) w[i] = q[i] * inv;
-  }
-}
 
 constexpr int kP2MChunk = 64;
 

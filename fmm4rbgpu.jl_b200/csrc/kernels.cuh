@@ -32,7 +32,9 @@ int compute_pavg_stretch(Ctx *ctx, const double *d_mom_aos, int64_t N, double *d
 // stretch in d_consts[3..5]; fills ctx tree buffers and ctx->{N,N0,ml,nc,...}.
 int build_tree(Ctx *ctx, const double *d_pos_aos, int64_t N, int64_t N0, const double *d_consts);
 // Particle records in tree order ("prec64": x,y,z,gamma,ux,uy,uz,0) and, for
-// the mixed form, leaf-local FP32 records ("prec32").
+// the mixed form, leaf-local FP32 records ("prec32": x,y,z,gamma,ux,uy,uz,0
+// relative to the leaf's box centre) with the low parts of the coordinates
+// ("prec32lo": x,y,z,0).
 // leafpos (optional): leaf cluster of every tree-order position (explicit trees).
 int gather_particles(Ctx *ctx, const double *d_pos_aos, const double *d_mom_aos, bool mixed,
                      const int *leafpos = nullptr);
@@ -44,6 +46,13 @@ int node_stride(int n);
 
 // ---------------------------------------------------------------- traverse.cu
 int build_lists(Ctx *ctx, double eta, const double *d_consts);
+// m2lu_* / p2pu_*: union of each list and its transpose with role flags
+// (bit 0: (t,s) in the list, bit 1: (s,t) in the list), grouped by target.
+int build_union_lists(Ctx *ctx);
+
+// ---------------------------------------------------------------- backward.cu
+// Adjoint of the saved FP64 forward; device AoS arrays in the caller's order.
+int run_backward(Ctx *ctx, const double *d_ge, const double *d_gb, double *d_gx, double *d_gu);
 
 // ---------------------------------------------------------------- interp.cu
 // P2M of leaves (leaf_ids null: all leaves of the tree) into "mom"; accumulate

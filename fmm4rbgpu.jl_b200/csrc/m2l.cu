@@ -10,7 +10,9 @@
 // bulk-copy (TMA) into a double buffer guarded by two mbarriers, so the next
 // source streams in while the current one is evaluated.  The kernel matrix is
 // generated on the fly; per-axis target-source offsets are hoisted so that one
-// evaluation costs three adds/FMAs for the denominator.  (The reference
+// evaluation costs three adds/FMAs for the denominator, and the E/B sums are
+// factored through per-source-node vectors packed once per source (below), so
+// that an evaluation accumulates with 10 FMAs.  (The reference
 // re-stages into one shared buffer without a barrier after the compute loop --
 // a write-after-read race; here the end-of-iteration barrier orders it.)
 //
@@ -46,18 +48,28 @@ __device__ __forceinline__ void kahan_add(float &sum, float &comp, float v) {
   sum = t;
 }
 
-template <int NDEG, bool MIXED>
+// Packed per-source-node data (x' = node - target centre):
+//   P0 = (Gamma, Gamma x', Gamma y', Gamma z'), P1 = (Mx, My, Mz, 0), P2 = M x x' (3), 0
+// so that, with s3 = d^{-3/2},
+//   E_a = sum s3 Gamma_b (x_a - x_b) = x_a' G - Q,     G = sum s3 Gamma_b,  Q = sum s3 Gamma_b x_b'
+//   B_a = sum s3 M_b x (x_a - x_b)   = W x x_a' - V,   W = sum s3 M_b,      V = sum s3 M_b x x_b'
+// and one evaluation costs the denominator (3), rsqrt, s3 (2) and 10 FMAs.
+// MASK: zero K at coincident nodes (R = 0), possible only for eta > 1/2.
+template <int NDEG, bool MIXED, bool MASK>
 __global__ void __launch_bounds__(M2LShape<NDEG>::BT)
     m2l_kernel(const int *__restrict__ ptr, const int *__restrict__ src, const double *__restrict__ nodes,
-               const void *__restrict__ mom_v, void *__restrict__ loc_v, const double *__restrict__ consts,
-               int accumulate, int *__restrict__ status) {
+               const double *__restrict__ bbox, const void *__restrict__ mom_v, void *__restrict__ loc_v,
+               const double *__restrict__ consts, int accumulate, int *__restrict__ status) {
   using S = M2LShape<NDEG>;
   constexpr int M = S::M, NN = S::NN, NS = S::NS, TPT = S::TPT, BT = S::BT;
   using T = typename std::conditional<MIXED, float, double>::type;
+  using T4 = typename std::conditional<MIXED, float4, double4>::type;
   constexpr int MOM_BYTES = 4 * NN * (int)sizeof(T);
-  constexpr int REC_BYTES = MOM_BYTES + NS * 8;  // moments then node coordinates
+  constexpr int REC_BYTES = MOM_BYTES + NS * 8;  // raw moments then node coordinates
   extern __shared__ __align__(16) unsigned char smem[];
+  T4 *pk = (T4 *)(smem + 2 * REC_BYTES);  // 3*NN packed entries
   __shared__ __align__(8) uint64_t bar[2];
+  __shared__ double s_sn[3 * M];           // source node offsets from the target centre
 
   const T *mom = (const T *)mom_v;
   T *loc = (T *)loc_v;
@@ -65,14 +77,16 @@ __global__ void __launch_bounds__(M2LShape<NDEG>::BT)
   const int t = blockIdx.x;
   const int p0 = ptr[t], np = ptr[t + 1] - p0;
   const double *tn = nodes + (int64_t)t * NS;
+  const double *tb = bbox + 6 * (int64_t)t;
+  const double cx = 0.5 * (tb[0] + tb[3]), cy = 0.5 * (tb[1] + tb[4]), cz = 0.5 * (tb[2] + tb[5]);
 
-  // accumulators: FP64 sums, or FP32 Kahan (sum, compensation) pairs
-  double acc[TPT][6];
-  float ks[TPT][6], kc[TPT][6];
+  // accumulators G, Q(3), W(3), V(3): FP64 sums, or FP32 Kahan (sum, compensation) pairs
+  double acc[TPT][10];
+  float ks[TPT][10], kc[TPT][10];
 #pragma unroll
   for (int q = 0; q < TPT; ++q)
 #pragma unroll
-    for (int c = 0; c < 6; ++c) {
+    for (int c = 0; c < 10; ++c) {
       acc[q][c] = 0.0;
       ks[q][c] = 0.f;
       kc[q][c] = 0.f;
@@ -93,7 +107,8 @@ __global__ void __launch_bounds__(M2LShape<NDEG>::BT)
       bulk_g2s(dst + MOM_BYTES, nodes + (int64_t)s * NS, NS * 8, &bar[bb]);
     };
     if (tid == 0) issue(0, 0);
-    const T px = (T)consts[0], py = (T)consts[1], pz = (T)consts[2];
+    const double pxd = consts[0], pyd = consts[1], pzd = consts[2];
+    const T px = (T)pxd, py = (T)pyd, pz = (T)pzd;
     for (int i = 0; i < np; ++i) {
       const int bb = i & 1;
       if (tid == 0 && i + 1 < np) {
@@ -101,76 +116,91 @@ __global__ void __launch_bounds__(M2LShape<NDEG>::BT)
         issue(i + 1, bb ^ 1);
       }
       const bool ok = mbar_wait_bounded(&bar[bb], (uint32_t)((i >> 1) & 1), status);
+      // pack the source's node data relative to the target centre
+      const T *G = (const T *)(smem + bb * REC_BYTES);
+      const double *SN = (const double *)(smem + bb * REC_BYTES + MOM_BYTES);
       if (ok) {
-        const T *G = (const T *)(smem + bb * REC_BYTES);
-        const T *MX = G + NN, *MY = G + 2 * NN, *MZ = G + 3 * NN;
-        const double *SN = (const double *)(smem + bb * REC_BYTES + MOM_BYTES);
+        for (int e = tid; e < 3 * M; e += BT) {
+          const int d = e / M;
+          s_sn[e] = SN[e] - (d == 0 ? cx : (d == 1 ? cy : cz));
+        }
+        for (int b = tid; b < NN; b += BT) {
+          const int bi = b % M, bj = (b / M) % M, bk = b / (M * M);
+          const T xb = (T)(SN[bi] - cx), yb = (T)(SN[M + bj] - cy), zb = (T)(SN[2 * M + bk] - cz);
+          const T g = G[b], m0 = G[NN + b], m1 = G[2 * NN + b], m2 = G[3 * NN + b];
+          T4 a, c, e;
+          a.x = g; a.y = g * xb; a.z = g * yb; a.w = g * zb;
+          c.x = m0; c.y = m1; c.z = m2; c.w = 0;
+          e.x = m1 * zb - m2 * yb; e.y = m2 * xb - m0 * zb; e.z = m0 * yb - m1 * xb; e.w = 0;
+          pk[3 * b] = a;
+          pk[3 * b + 1] = c;
+          pk[3 * b + 2] = e;
+        }
+      }
+      __syncthreads();
+      if (ok) {
 #pragma unroll
         for (int q = 0; q < TPT; ++q) {
           const int a = tid + q * BT;
           if (a < NN) {
             const int ai = a % M, aj = (a / M) % M, ak = a / (M * M);
-            const double tx = tn[ai], ty = tn[M + aj], tz = tn[2 * M + ak];
-            T rx[M], prx[M], rx2[M];
+            const double tx = tn[ai] - cx, ty = tn[M + aj] - cy, tz = tn[2 * M + ak] - cz;
+            T prx[M], rx2[M];
 #pragma unroll
             for (int bi = 0; bi < M; ++bi) {
-              rx[bi] = (T)(tx - SN[bi]);
-              prx[bi] = px * rx[bi];
-              rx2[bi] = rx[bi] * rx[bi];
+              const T rx = (T)(tx - s_sn[bi]);
+              prx[bi] = px * rx;
+              rx2[bi] = rx * rx;
             }
-            T e0 = 0, e1 = 0, e2 = 0, b0 = 0, b1 = 0, b2 = 0;
+            T g0 = 0, q0 = 0, q1 = 0, q2 = 0, w0 = 0, w1 = 0, w2 = 0, v0 = 0, v1 = 0, v2 = 0;
 #pragma unroll 1
             for (int bk = 0; bk < M; ++bk) {
-              const T rz = (T)(tz - SN[2 * M + bk]);
+              const T rz = (T)(tz - s_sn[2 * M + bk]);
               const T prz = pz * rz;
               const T rz2 = rz * rz + (T)kEps64;
 #pragma unroll
               for (int bj = 0; bj < M; ++bj) {
-                const T ry = (T)(ty - SN[M + bj]);
+                const T ry = (T)(ty - s_sn[M + bj]);
                 const T P = py * ry + prz;
                 const T A = ry * ry + rz2;
-                const int b0i = M * (bj + M * bk);
+                const T4 *pb = pk + 3 * M * (bj + M * bk);
 #pragma unroll
                 for (int bi = 0; bi < M; ++bi) {
                   const T tt = P + prx[bi];
-                  const T u = A + rx2[bi];
-                  const T d = tt * tt + u;
+                  const T d = tt * tt + (A + rx2[bi]);
                   T s;
                   if constexpr (MIXED)
                     s = rsqrt_approx(d);
                   else
                     s = rsqrt(d);
-                  const T s3 = s * s * s;
-                  const T g = G[b0i + bi] * s3;
-                  e0 += g * rx[bi];
-                  e1 += g * ry;
-                  e2 += g * rz;
-                  const T hx = MX[b0i + bi] * s3, hy = MY[b0i + bi] * s3, hz = MZ[b0i + bi] * s3;
-                  b0 += hy * rz - hz * ry;
-                  b1 += hz * rx[bi] - hx * rz;
-                  b2 += hx * ry - hy * rx[bi];
+                  T s3 = s * s * s;
+                  if constexpr (MASK) s3 = d > (T)kEps64 ? s3 : (T)0;
+                  const T4 a4 = pb[3 * bi], m4 = pb[3 * bi + 1], c4 = pb[3 * bi + 2];
+                  g0 += s3 * a4.x;
+                  q0 += s3 * a4.y;
+                  q1 += s3 * a4.z;
+                  q2 += s3 * a4.w;
+                  w0 += s3 * m4.x;
+                  w1 += s3 * m4.y;
+                  w2 += s3 * m4.z;
+                  v0 += s3 * c4.x;
+                  v1 += s3 * c4.y;
+                  v2 += s3 * c4.z;
                 }
               }
             }
-            if constexpr (MIXED) {
-              kahan_add(ks[q][0], kc[q][0], e0);
-              kahan_add(ks[q][1], kc[q][1], e1);
-              kahan_add(ks[q][2], kc[q][2], e2);
-              kahan_add(ks[q][3], kc[q][3], b0);
-              kahan_add(ks[q][4], kc[q][4], b1);
-              kahan_add(ks[q][5], kc[q][5], b2);
-            } else {
-              acc[q][0] += e0;
-              acc[q][1] += e1;
-              acc[q][2] += e2;
-              acc[q][3] += b0;
-              acc[q][4] += b1;
-              acc[q][5] += b2;
+            const T part[10] = {g0, q0, q1, q2, w0, w1, w2, v0, v1, v2};
+#pragma unroll
+            for (int c = 0; c < 10; ++c) {
+              if constexpr (MIXED)
+                kahan_add(ks[q][c], kc[q][c], part[c]);
+              else
+                acc[q][c] += part[c];
             }
           }
         }
       }
-      __syncthreads();  // everyone is done with buffer bb before it is refilled
+      __syncthreads();  // the packed data and buffer bb are rewritten later
     }
   }
   T *out = loc + (int64_t)t * 6 * NN;
@@ -178,35 +208,48 @@ __global__ void __launch_bounds__(M2LShape<NDEG>::BT)
   for (int q = 0; q < TPT; ++q) {
     const int a = tid + q * BT;
     if (a < NN) {
+      const int ai = a % M, aj = (a / M) % M, ak = a / (M * M);
+      const double xa = tn[ai] - cx, ya = tn[M + aj] - cy, za = tn[2 * M + ak] - cz;
+      double v[10];
+#pragma unroll
+      for (int c = 0; c < 10; ++c) v[c] = MIXED ? (double)ks[q][c] - (double)kc[q][c] : acc[q][c];
+      // E = x' G - Q ; B = W x x' - V
+      const double f[6] = {xa * v[0] - v[1], ya * v[0] - v[2], za * v[0] - v[3],
+                           (v[5] * za - v[6] * ya) - v[7], (v[6] * xa - v[4] * za) - v[8],
+                           (v[4] * ya - v[5] * xa) - v[9]};
 #pragma unroll
       for (int c = 0; c < 6; ++c) {
-        T v;
-        if constexpr (MIXED)
-          v = ks[q][c];
-        else
-          v = acc[q][c];
-        if (accumulate) v += out[c * NN + a];
-        out[c * NN + a] = v;
+        T o = (T)f[c];
+        if (accumulate) o += out[c * NN + a];
+        out[c * NN + a] = o;
       }
     }
   }
 }
 
-template <int NDEG, bool MIXED>
+template <int NDEG, bool MIXED, bool MASK>
 int launch_m2l_t(Ctx *ctx, bool accumulate) {
   using S = M2LShape<NDEG>;
   using T = typename std::conditional<MIXED, float, double>::type;
   const int rec = 4 * S::NN * (int)sizeof(T) + S::NS * 8;
-  const int smem = 2 * rec;
-  auto kern = m2l_kernel<NDEG, MIXED>;
+  const int smem = 2 * rec + 3 * S::NN * 4 * (int)sizeof(T);
+  auto kern = m2l_kernel<NDEG, MIXED, MASK>;
   FMM_TRY(opt_in_smem(ctx, kern, smem));
   if (ctx->nc > 0)
     kern<<<(unsigned)ctx->nc, S::BT, smem, ctx->stream>>>(
-        ctx->get<int>("m2l_ptr"), ctx->get<int>("m2l_src"), ctx->get<double>("nodes"),
+        ctx->get<int>("m2l_ptr"), ctx->get<int>("m2l_src"), ctx->get<double>("nodes"), ctx->get<double>("bbox"),
         MIXED ? (const void *)ctx->get<float>("mom32") : (const void *)ctx->get<double>("mom64"),
         MIXED ? (void *)ctx->get<float>("loc32") : (void *)ctx->get<double>("loc64"), ctx->get<double>("consts"),
         accumulate ? 1 : 0, ctx->d_status);
   return ctx->check_launch("m2l_kernel");
+}
+
+template <int NDEG>
+int launch_m2l_n(Ctx *ctx, bool mixed, bool accumulate) {
+  // coincident target/source nodes need eta > 1/2 (admissible: max(r1,r2) < eta R)
+  const bool mask = !(ctx->eta <= 0.5);
+  if (mixed) return mask ? launch_m2l_t<NDEG, true, true>(ctx, accumulate) : launch_m2l_t<NDEG, true, false>(ctx, accumulate);
+  return mask ? launch_m2l_t<NDEG, false, true>(ctx, accumulate) : launch_m2l_t<NDEG, false, false>(ctx, accumulate);
 }
 
 }  // namespace
@@ -214,7 +257,7 @@ int launch_m2l_t(Ctx *ctx, bool accumulate) {
 int launch_m2l(Ctx *ctx, int n, bool mixed, bool accumulate) {
 #define FMM_M2L_CASE(D) \
   case D:               \
-    return mixed ? launch_m2l_t<D, true>(ctx, accumulate) : launch_m2l_t<D, false>(ctx, accumulate);
+    return launch_m2l_n<D>(ctx, mixed, accumulate);
   switch (n) {
     FMM_M2L_CASE(1)
     FMM_M2L_CASE(2)

@@ -9,6 +9,8 @@
 // outputs at offsets from a block scan, so every step is deterministic.  The
 // set of emitted pairs equals the DFS's.  Both lists are then radix-sorted by
 // (target, source) and grouped into CSR pointers over all clusters.
+#include <string>
+
 #include "device_util.cuh"
 #include "kernels.cuh"
 
@@ -156,6 +158,32 @@ __global__ void p2p_work_kernel(const uint64_t *__restrict__ keys, int64_t n, in
   if (threadIdx.x == 0 && s) atomicAdd(out, s);
 }
 
+// Union of a sorted pair list and its transpose: entry (t,s) with bit 61 if
+// (t,s) is in the list and bit 62 if (s,t) is.
+__global__ void union_fill_kernel(const uint64_t *__restrict__ keys, int64_t n, int bits, uint64_t *__restrict__ out) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint64_t k = keys[i], mask = ((uint64_t)1 << bits) - 1;
+  out[i] = k | ((uint64_t)1 << 61);
+  out[n + i] = (((k & mask) << bits) | (k >> bits)) | ((uint64_t)1 << 62);
+}
+
+__global__ void union_head_kernel(const uint64_t *__restrict__ u, int64_t n, uint64_t low, int *__restrict__ head) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  head[i] = (i == 0 || (u[i] & low) != (u[i - 1] & low)) ? 1 : 0;
+}
+
+__global__ void union_compact_kernel(const uint64_t *__restrict__ u, int64_t n, uint64_t low, const int *__restrict__ head,
+                                     const int *__restrict__ pos, uint64_t *__restrict__ ukeys, uint8_t *__restrict__ uflag) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || !head[i]) return;
+  uint64_t f = u[i] >> 61;
+  if (i + 1 < n && (u[i + 1] & low) == (u[i] & low)) f |= u[i + 1] >> 61;
+  ukeys[pos[i]] = u[i] & low;
+  uflag[pos[i]] = (uint8_t)f;
+}
+
 // Grow a device buffer keeping its first `used` bytes.
 int grow_keep(Ctx *ctx, const char *name, size_t used, size_t need, void **out) {
   auto it = ctx->bufs.find(name);
@@ -204,7 +232,52 @@ int sort_and_group(Ctx *ctx, const char *keys_name, const char *alt_name, const 
   return ctx->check_launch("sort_and_group", n > 0 ? 2 : 1);
 }
 
+int build_union(Ctx *ctx, const char *keys_name, int64_t n, const char *prefix) {
+  const int bits = ctx->list_bits;
+  const int64_t n2 = 2 * n;
+  uint64_t *u, *ua;
+  int *head, *pos;
+  FMM_TRY(ctx->ensure("union_u", n2, &u));
+  FMM_TRY(ctx->ensure("union_ua", n2, &ua));
+  FMM_TRY(ctx->ensure("union_head", n2, &head));
+  FMM_TRY(ctx->ensure("union_pos", n2, &pos));
+  if (n > 0) union_fill_kernel<<<ceil_div(n, 256), 256, 0, ctx->stream>>>(ctx->get<uint64_t>(keys_name), n, bits, u);
+  FMM_TRY(ctx->check_launch("union_fill_kernel", n > 0 ? 1 : 0));
+  bool alt = false;
+  FMM_TRY(radix_sort(ctx, u, ua, nullptr, nullptr, n2, 2 * bits, &alt));
+  const uint64_t *us = alt ? ua : u;
+  const uint64_t low = ((uint64_t)1 << (2 * bits)) - 1;
+  int64_t nu = 0;
+  if (n2 > 0) {
+    union_head_kernel<<<ceil_div(n2, 256), 256, 0, ctx->stream>>>(us, n2, low, head);
+    FMM_TRY(ctx->check_launch("union_head_kernel"));
+    FMM_TRY(exclusive_scan_i32(ctx, head, pos, n2, &nu));
+  }
+  const std::string kn = std::string(prefix) + "_keys", fn = std::string(prefix) + "_flag";
+  const std::string pn = std::string(prefix) + "_ptr", sn = std::string(prefix) + "_src";
+  uint64_t *uk;
+  uint8_t *uf;
+  int *ptr, *src;
+  FMM_TRY(ctx->ensure(kn.c_str(), nu, &uk));
+  FMM_TRY(ctx->ensure(fn.c_str(), nu, &uf));
+  FMM_TRY(ctx->ensure(pn.c_str(), ctx->nc + 1, &ptr));
+  FMM_TRY(ctx->ensure(sn.c_str(), nu, &src));
+  if (n2 > 0) {
+    union_compact_kernel<<<ceil_div(n2, 256), 256, 0, ctx->stream>>>(us, n2, low, head, pos, uk, uf);
+    FMM_TRY(ctx->check_launch("union_compact_kernel"));
+  }
+  csr_kernel<<<ceil_div(ctx->nc + 1, 256), 256, 0, ctx->stream>>>(uk, nu, bits, ctx->nc, ptr);
+  if (nu > 0) src_kernel<<<ceil_div(nu, 256), 256, 0, ctx->stream>>>(uk, nu, bits, src);
+  return ctx->check_launch("union csr", nu > 0 ? 2 : 1);
+}
+
 }  // namespace
+
+int build_union_lists(Ctx *ctx) {
+  FMM_TRY(build_union(ctx, "m2l_keys", ctx->nm2l, "m2lu"));
+  FMM_TRY(build_union(ctx, "p2p_keys", ctx->np2p, "p2pu"));
+  return FMMB200_OK;
+}
 
 int build_lists(Ctx *ctx, double eta, const double *d_consts) {
   const int64_t nc = ctx->nc;

@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "device_util.cuh"
+#include "interp_util.cuh"
 #include "kernels.cuh"
 
 namespace fmmb200 {
@@ -291,7 +292,7 @@ __global__ void gather64_kernel(int N, const uint32_t *__restrict__ perm, const 
 __global__ void gather32_kernel(int ml, int N, const uint32_t *__restrict__ perm,
                                 const double *__restrict__ pos, const double *__restrict__ mom,
                                 const double *__restrict__ bbox, const int *__restrict__ leafpos,
-                                float *__restrict__ rec) {
+                                float *__restrict__ rec, float *__restrict__ rec_lo) {
   int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= N) return;
   int lo, hi;
@@ -301,15 +302,16 @@ __global__ void gather32_kernel(int ml, int N, const uint32_t *__restrict__ perm
   double cx = 0.5 * (bb[0] + bb[3]), cy = 0.5 * (bb[1] + bb[4]), cz = 0.5 * (bb[2] + bb[5]);
   double ux = mom[3 * p], uy = mom[3 * p + 1], uz = mom[3 * p + 2];
   double g = sqrt(1.0 + (ux * ux + uy * uy + uz * uz));
+  const double lx = pos[3 * p] - cx, ly = pos[3 * p + 1] - cy, lz = pos[3 * p + 2] - cz;
+  const float hx = (float)lx, hy = (float)ly, hz = (float)lz;
   float4 *r = reinterpret_cast<float4 *>(rec + 8 * (int64_t)j);
-  r[0] = make_float4((float)(pos[3 * p] - cx), (float)(pos[3 * p + 1] - cy), (float)(pos[3 * p + 2] - cz),
-                     (float)g);
+  r[0] = make_float4(hx, hy, hz, (float)g);
   r[1] = make_float4((float)ux, (float)uy, (float)uz, 0.0f);
+  // hi + lo reproduces the local coordinate to ~2^-48 relative: P2P forms the
+  // difference of two nearby particles exactly from the hi parts (Sterbenz)
+  reinterpret_cast<float4 *>(rec_lo)[j] = make_float4((float)(lx - (double)hx), (float)(ly - (double)hy),
+                                                  (float)(lz - (double)hz), 0.0f);
 }
-
-struct ChebT {
-  double t[kMaxNodes1D];
-};
 
 // nodes[c][d][i] = a + (cos(pi*i/n) + 1)/2 * (b - a)  (barylg.jl:25-27, 0-based i)
 __global__ void nodes_kernel(int64_t nc, int M, int NS, ChebT ct, const double *__restrict__ bbox,
@@ -509,10 +511,11 @@ int gather_particles(Ctx *ctx, const double *d_pos, const double *d_mom, bool mi
   gather64_kernel<<<ceil_div(N, TB), TB, 0, ctx->stream>>>(N, ctx->get<uint32_t>("perm"), d_pos, d_mom, rec);
   FMM_TRY(ctx->check_launch("gather64_kernel"));
   if (mixed) {
-    float *r32;
+    float *r32, *lo32;
     FMM_TRY(ctx->ensure("prec32", 8 * (int64_t)N, &r32));
+    FMM_TRY(ctx->ensure("prec32lo", 4 * (int64_t)N, &lo32));
     gather32_kernel<<<ceil_div(N, TB), TB, 0, ctx->stream>>>(ctx->ml, N, ctx->get<uint32_t>("perm"), d_pos, d_mom,
-                                                              ctx->get<double>("bbox"), leafpos, r32);
+                                                              ctx->get<double>("bbox"), leafpos, r32, lo32);
     FMM_TRY(ctx->check_launch("gather32_kernel"));
   }
   return FMMB200_OK;
