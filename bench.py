@@ -39,6 +39,8 @@ sys.path.insert(0, ROOT)
 
 import numpy as np  # noqa: E402
 
+from fmmb200 import replicas  # noqa: E402
+
 METRIC = "particles/s at N=2^24: FP32 form vs FP64 plain at stated rel err; fwd+bwd time"
 SM_COUNT_NOTE = "B200, 148 SMs"
 
@@ -146,37 +148,20 @@ def model_flops(st: dict, n: int, N: int) -> float:
 def dist_setup(args):
     import torch
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    world, rank, local = replicas.env_ranks()
     if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
+        replicas.init("nccl", local)
     elif torch.cuda.is_available():
         torch.cuda.set_device(0)
     return world, rank, local
 
 
 def barrier(world):
-    if world > 1:
-        import torch.distributed as dist
-
-        dist.barrier()
+    replicas.barrier(world)
 
 
 def max_over_ranks(world, v: float) -> float:
-    if world == 1:
-        return v
-    import torch
-    import torch.distributed as dist
-
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    return replicas.max_over_ranks(world, v, device="cuda")
 
 
 # ---------------------------------------------------------------------------- reference arm
@@ -346,7 +331,7 @@ def run_ours(args, world, rank, local):
         ev1.synchronize()
         ms_e2e = max_over_ranks(world, ev0.elapsed_time(ev1) / args.steps)
         assert torch.equal(eh, E.cpu()), "host-pointer and device-pointer paths must agree"
-        e2e = {"value": world * N / (ms_e2e * 1e-3), "unit": "particles/s", "ms_per_step": ms_e2e,
+        e2e = {"value": replicas.aggregate_rate(world, N, ms_e2e), "unit": "particles/s", "ms_per_step": ms_e2e,
                "h2d_bytes_per_step": 2 * 24 * N, "d2h_bytes_per_step": 2 * 24 * N}
 
     cpu = None
@@ -358,12 +343,12 @@ def run_ours(args, world, rank, local):
         stages64 = {k: st64[k] for k in ("ms_tree", "ms_upward", "ms_lists", "ms_m2l", "ms_p2p", "ms_downward")}
         mf = model_flops(st, args.n, N)
         out = {
-            "metric": METRIC, "value": world * N / (ms_mixed * 1e-3), "unit": "particles/s", "n_gpus": world,
+            "metric": METRIC, "value": replicas.aggregate_rate(world, N, ms_mixed), "unit": "particles/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_mixed, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic: seeded Gaussian bunch per rank (the reference benchmarks no public dataset)",
             "config": workload(args),
-            "fp64": {"value": world * N / (ms_fp64 * 1e-3), "unit": "particles/s", "ms_per_step": ms_fp64,
+            "fp64": {"value": replicas.aggregate_rate(world, N, ms_fp64), "unit": "particles/s", "ms_per_step": ms_fp64,
                      "stages_ms": stages64, "mixed_speedup": ms_fp64 / ms_mixed},
             "accuracy": acc,
             "stages_ms": stages,
@@ -385,8 +370,7 @@ def run_ours(args, world, rank, local):
 def main():
     args = parse()
     if args.impl == "reference":
-        world = int(os.environ.get("WORLD_SIZE", "1"))
-        rank = int(os.environ.get("RANK", "0"))
+        world, rank, _ = replicas.env_ranks()
         run_reference(args, world, rank)
         return
     world, rank, local = dist_setup(args)

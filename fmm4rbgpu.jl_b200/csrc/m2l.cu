@@ -80,13 +80,13 @@ __global__ void __launch_bounds__(M2LShape<NDEG>::BT)
   const double *tb = bbox + 6 * (int64_t)t;
   const double cx = 0.5 * (tb[0] + tb[3]), cy = 0.5 * (tb[1] + tb[4]), cz = 0.5 * (tb[2] + tb[5]);
 
-  // accumulators G, Q(3), W(3), V(3): FP64 sums, or FP32 Kahan (sum, compensation) pairs
-  double acc[TPT][10];
-  float ks[TPT][10], kc[TPT][10];
+  // E(3), B(3) accumulated over source pairs: FP64 sums, or FP32 Kahan (sum, compensation)
+  double acc[TPT][6];
+  float ks[TPT][6], kc[TPT][6];
 #pragma unroll
   for (int q = 0; q < TPT; ++q)
 #pragma unroll
-    for (int c = 0; c < 10; ++c) {
+    for (int c = 0; c < 6; ++c) {
       acc[q][c] = 0.0;
       ks[q][c] = 0.f;
       kc[q][c] = 0.f;
@@ -189,9 +189,13 @@ __global__ void __launch_bounds__(M2LShape<NDEG>::BT)
                 }
               }
             }
-            const T part[10] = {g0, q0, q1, q2, w0, w1, w2, v0, v1, v2};
+            // this source's E and B at the node: E = x' G - Q, B = W x x' - V.  Folding per
+            // source keeps the cancellation between sources in the compensated sum.
+            const T xa = (T)tx, ya = (T)ty, za = (T)tz;
+            const T part[6] = {xa * g0 - q0, ya * g0 - q1, za * g0 - q2,
+                               (w1 * za - w2 * ya) - v0, (w2 * xa - w0 * za) - v1, (w0 * ya - w1 * xa) - v2};
 #pragma unroll
-            for (int c = 0; c < 10; ++c) {
+            for (int c = 0; c < 6; ++c) {
               if constexpr (MIXED)
                 kahan_add(ks[q][c], kc[q][c], part[c]);
               else
@@ -208,18 +212,9 @@ __global__ void __launch_bounds__(M2LShape<NDEG>::BT)
   for (int q = 0; q < TPT; ++q) {
     const int a = tid + q * BT;
     if (a < NN) {
-      const int ai = a % M, aj = (a / M) % M, ak = a / (M * M);
-      const double xa = tn[ai] - cx, ya = tn[M + aj] - cy, za = tn[2 * M + ak] - cz;
-      double v[10];
-#pragma unroll
-      for (int c = 0; c < 10; ++c) v[c] = MIXED ? (double)ks[q][c] - (double)kc[q][c] : acc[q][c];
-      // E = x' G - Q ; B = W x x' - V
-      const double f[6] = {xa * v[0] - v[1], ya * v[0] - v[2], za * v[0] - v[3],
-                           (v[5] * za - v[6] * ya) - v[7], (v[6] * xa - v[4] * za) - v[8],
-                           (v[4] * ya - v[5] * xa) - v[9]};
 #pragma unroll
       for (int c = 0; c < 6; ++c) {
-        T o = (T)f[c];
+        T o = MIXED ? (T)((double)ks[q][c] - (double)kc[q][c]) : (T)acc[q][c];
         if (accumulate) o += out[c * NN + a];
         out[c * NN + a] = o;
       }
