@@ -7,6 +7,7 @@
 // the sources over `splits` slices; each CTA streams its slice through shared
 // memory tiles and writes one partial per target, and a second kernel adds the
 // partials in slice order, so the result is deterministic.
+#include <mutex>
 #include <vector>
 
 #include "device_util.cuh"
@@ -15,6 +16,18 @@
 using namespace fmmb200;
 
 namespace {
+
+// Scratch of fmmb200_direct_noalloc: 6 partial sums per (target, source slice)
+// slot, for at most kNoAllocSlots slots (3 MiB).  Every GPU that loads the
+// library holds this array until the process exits.
+constexpr int64_t kNoAllocSlots = 65536;
+__device__ __align__(256) double g_noalloc_scratch[6 * kNoAllocSlots];
+
+// Device address of g_noalloc_scratch per device (the host-side symbol is a
+// stand-in, not a device address), filled once per device.
+constexpr int kMaxDevices = 64;
+double *g_noalloc_ptr[kMaxDevices] = {};
+std::mutex g_noalloc_mutex;
 
 constexpr int kDirThreads = 128;
 constexpr int kDirTile = 256;
@@ -115,11 +128,19 @@ __global__ void fma_peak_kernel(T *out, int iters, T a, T b) {
   if (r == (T)-1.2345) out[threadIdx.x] = r;  // keeps the chains alive
 }
 
-int run_direct(Ctx *ctx, int64_t N, const double *d_pos, const double *d_mom, double charge, double lambda,
-               int64_t ntarget, const int64_t *d_targets, double *d_e, double *d_b) {
+int pick_splits(int64_t N, int64_t ntarget, int64_t max_slots) {
   int splits = 1;
   const int64_t tblocks = (ntarget + kDirThreads - 1) / kDirThreads;
-  while (tblocks * splits < 148 * 8 && splits < 1024 && (N / (splits * 2)) >= kDirTile) splits *= 2;
+  while (tblocks * splits < 148 * 8 && splits < 1024 && (N / (splits * 2)) >= kDirTile &&
+         ntarget * splits * 2 <= max_slots)
+    splits *= 2;
+  return splits;
+}
+
+int run_direct(Ctx *ctx, int64_t N, const double *d_pos, const double *d_mom, double charge, double lambda,
+               int64_t ntarget, const int64_t *d_targets, double *d_e, double *d_b) {
+  const int splits = pick_splits(N, ntarget, INT64_MAX);
+  const int64_t tblocks = (ntarget + kDirThreads - 1) / kDirThreads;
   double *part;
   FMM_TRY(ctx->ensure("direct_part", 6 * ntarget * splits, &part));
   dim3 grid((unsigned)tblocks, (unsigned)splits);
@@ -170,6 +191,42 @@ int fmmb200_direct(fmmb200_ctx *ctx, int64_t npar, const double *positions, cons
   FMM_CUDA_TRY(ctx, cudaMemcpyAsync(efields, de, sizeof(double) * 3 * nt, cudaMemcpyDeviceToHost, ctx->stream));
   FMM_CUDA_TRY(ctx, cudaMemcpyAsync(bfields, db, sizeof(double) * 3 * nt, cudaMemcpyDeviceToHost, ctx->stream));
   return ctx->sync();
+}
+
+int fmmb200_direct_noalloc(int64_t npar, const double *d_positions, const double *d_momenta, double charge,
+                           double lambda, int64_t ntarget, const int64_t *d_targets, double *d_efields,
+                           double *d_bfields, void *stream) {
+  if (npar < 1 || ntarget < 1 || !d_positions || !d_momenta || !d_efields || !d_bfields || !(lambda != 0.0))
+    return FMMB200_ERR_INVALID_ARGUMENT;
+  if (ntarget > kNoAllocSlots) return FMMB200_ERR_CAPACITY;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+    cudaGetLastError();
+    return FMMB200_ERR_CUDA;
+  }
+  double *scratch;
+  {
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev]) {
+      // once per device, with that device current: the device address of the array
+      double *p = nullptr;
+      if (cudaGetSymbolAddress((void **)&p, g_noalloc_scratch) != cudaSuccess || !p) {
+        cudaGetLastError();
+        return FMMB200_ERR_CUDA;
+      }
+      g_noalloc_ptr[dev] = p;
+    }
+    scratch = g_noalloc_ptr[dev];
+  }
+  const int splits = pick_splits(npar, ntarget, kNoAllocSlots);
+  const int64_t tblocks = (ntarget + kDirThreads - 1) / kDirThreads;
+  cudaStream_t st = (cudaStream_t)stream;
+  dim3 grid((unsigned)tblocks, (unsigned)splits);
+  direct_partial_kernel<<<grid, kDirThreads, 0, st>>>(npar, d_positions, d_momenta, ntarget, d_targets, splits, scratch);
+  direct_reduce_kernel<<<ceil_div(ntarget, 256), 256, 0, st>>>(ntarget, splits, scratch, kRe * charge / lambda,
+                                                               d_efields, d_bfields);
+  if (cudaGetLastError() != cudaSuccess) return FMMB200_ERR_CUDA;
+  return FMMB200_OK;
 }
 
 int fmmb200_measure_fma_peak(fmmb200_ctx *ctx, double *fp64_tflops, double *fp32_tflops) {

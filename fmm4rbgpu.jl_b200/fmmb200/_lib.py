@@ -29,6 +29,7 @@ ERR_CUDA = 3
 ERR_TREE_SHAPE = 4
 ERR_NO_STATE = 5
 ERR_DEVICE = 6
+ERR_CAPACITY = 7
 
 PRECISION_FP64 = 0
 PRECISION_MIXED = 1
@@ -99,6 +100,7 @@ SIGNATURES = {
     "fmmb200_direct": (ctypes.c_int, [c_vp, c_i64, p_f64, p_f64, c_f64, c_f64, c_i64, p_i64, p_f64, p_f64]),
     "fmmb200_direct_device": (ctypes.c_int, [c_vp, c_i64, c_vp, c_vp, c_f64, c_f64, c_i64, c_vp, c_vp, c_vp]),
     "fmmb200_measure_fma_peak": (ctypes.c_int, [c_vp, p_f64, p_f64]),
+    "fmmb200_direct_noalloc": (ctypes.c_int, [c_i64, c_vp, c_vp, c_f64, c_f64, c_i64, c_vp, c_vp, c_vp, c_vp]),
 }
 
 

@@ -43,6 +43,7 @@ extern "C" {
 #define FMMB200_ERR_TREE_SHAPE 4   /* a leaf would occur above the maximum level */
 #define FMMB200_ERR_NO_STATE 5     /* no forward state saved in the context */
 #define FMMB200_ERR_DEVICE 6       /* a kernel raised its device status word */
+#define FMMB200_ERR_CAPACITY 7     /* larger than a fixed-size scratch array allows */
 
 #define FMMB200_PRECISION_FP64 0   /* plain FP64 path (the drop-in) */
 #define FMMB200_PRECISION_MIXED 1  /* FP32 arithmetic, compensated sums, FP64 geometry */
@@ -186,6 +187,26 @@ int fmmb200_direct(fmmb200_ctx *ctx, int64_t npar, const double *positions, cons
 int fmmb200_direct_device(fmmb200_ctx *ctx, int64_t npar, const double *d_positions,
                           const double *d_momenta, double charge, double lambda, int64_t ntarget,
                           const int64_t *d_targets, double *d_efields, double *d_bfields);
+/* The FP64 direct sum of fmmb200_direct_device without allocating anything: no
+ * context, no cudaMalloc/cudaFree, no allocating library call (no counterpart in
+ * the reference).  It is for callers that cannot let a library allocate device
+ * memory: code whose device memory is owned by its own pool allocator (CUDA.jl's
+ * pool, a framework that reserved the GPU up front), where a private cudaMalloc
+ * may fail or fragment that pool, and loops in which the implicit device
+ * synchronisation of cudaMalloc/cudaFree is not acceptable.  The caller passes
+ * device inputs and outputs (d_targets: ntarget particle indices, NULL =
+ * particles 0..ntarget-1) and a cudaStream_t (NULL = default stream); the call is
+ * asynchronous on it.
+ * Scratch: a file-scope __device__ array of 6*65536 doubles (3 MiB), held by every
+ * GPU that loads the library until the process exits.  ntarget > 65536 returns
+ * FMMB200_ERR_CAPACITY.  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress) with that device current; make that first call
+ * before any stream capture.  All calls share the array and it keeps the last
+ * call's contents (each call writes every slot it reads); calls that overlap on
+ * the GPU, e.g. on different streams, race on it. */
+int fmmb200_direct_noalloc(int64_t npar, const double *d_positions, const double *d_momenta,
+                           double charge, double lambda, int64_t ntarget, const int64_t *d_targets,
+                           double *d_efields, double *d_bfields, void *stream);
 /* Measured CUDA-core FMA throughput (TFLOP/s, 2 flops per FMA) of the device:
  * the roofline denominators of the M2L / P2P kernels. */
 int fmmb200_measure_fma_peak(fmmb200_ctx *ctx, double *fp64_tflops, double *fp32_tflops);
