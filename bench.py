@@ -292,13 +292,15 @@ def run_ours(args, world, rank, local):
     # roofline of the dominant kernel (M2L) against the measured CUDA-core FMA peak
     p64 = ctypes.c_double()
     p32 = ctypes.c_double()
-    ctx._check(L.fmmb200_measure_fma_peak(ctx.handle, ctypes.byref(p64), ctypes.byref(p32)))
+    p2 = ctypes.c_double()
+    ctx._check(L.fmmb200_measure_fma_peak(ctx.handle, ctypes.byref(p64), ctypes.byref(p32), ctypes.byref(p2)))
     m2l_flops = 41.0 * st["m2l_kernel_evals"]
     ach32 = m2l_flops / (st["ms_m2l"] * 1e-3) / 1e12 if st["ms_m2l"] > 0 else 0.0
     ach64 = 41.0 * st64["m2l_kernel_evals"] / (st64["ms_m2l"] * 1e-3) / 1e12 if st64["ms_m2l"] > 0 else 0.0
     roof = {"kernel": "m2l_kernel<4, mixed>", "bound": "fp32", "achieved": ach32, "peak": p32.value,
             "unit": "TFLOP/s", "frac": ach32 / p32.value if p32.value else None, "traffic": None,
             "peak_source": "measured FP32 FMA throughput (fmmb200_measure_fma_peak) on this GPU",
+            "peak_fp32x2_measured": p2.value,
             "flops_per_launch": m2l_flops, "ms_per_launch": st["ms_m2l"],
             "fp64": {"kernel": "m2l_kernel<4, fp64>", "achieved": ach64, "peak": p64.value,
                      "frac": ach64 / p64.value if p64.value else None, "ms_per_launch": st64["ms_m2l"]}}

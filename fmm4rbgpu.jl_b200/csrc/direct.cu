@@ -137,6 +137,24 @@ int pick_splits(int64_t N, int64_t ntarget, int64_t max_slots) {
   return splits;
 }
 
+// Packed FP32x2 FMA chains (Blackwell FFMA2: two FMAs per lane per instruction).
+__global__ void fma2_peak_kernel(float *out, int iters, float a, float b) {
+  const float2 A = make_float2(a, a), Bv = make_float2(b, b);
+  float2 x[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) x[k] = make_float2((float)threadIdx.x * 1e-7f + 1e-3f * k, 2e-3f * k);
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int k = 0; k < 8; ++k) x[k] = __ffma2_rn(x[k], A, Bv);
+  }
+  float r = 0.f;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) r += x[k].x + x[k].y;
+  if (r == -1.2345f) out[threadIdx.x] = r;
+}
+
 int run_direct(Ctx *ctx, int64_t N, const double *d_pos, const double *d_mom, double charge, double lambda,
                int64_t ntarget, const int64_t *d_targets, double *d_e, double *d_b) {
   const int splits = pick_splits(N, ntarget, INT64_MAX);
@@ -229,7 +247,8 @@ int fmmb200_direct_noalloc(int64_t npar, const double *d_positions, const double
   return FMMB200_OK;
 }
 
-int fmmb200_measure_fma_peak(fmmb200_ctx *ctx, double *fp64_tflops, double *fp32_tflops) {
+int fmmb200_measure_fma_peak(fmmb200_ctx *ctx, double *fp64_tflops, double *fp32_tflops,
+                             double *fp32x2_tflops) {
   if (!ctx) return FMMB200_ERR_INVALID_ARGUMENT;
   cudaSetDevice(ctx->device);
   int nsm = 148;
@@ -242,7 +261,7 @@ int fmmb200_measure_fma_peak(fmmb200_ctx *ctx, double *fp64_tflops, double *fp32
   cudaEventCreate(&a);
   cudaEventCreate(&b);
   const int threads = 256, blocks = nsm * 8;
-  double best64 = 0, best32 = 0;
+  double best64 = 0, best32 = 0, best2 = 0;
   for (int rep = 0; rep < 3; ++rep) {
     const int it64 = 4096, it32 = 16384;
     cudaEventRecord(a, ctx->stream);
@@ -260,12 +279,20 @@ int fmmb200_measure_fma_peak(fmmb200_ctx *ctx, double *fp64_tflops, double *fp32
     cudaEventElapsedTime(&ms, a, b);
     const double fl32 = 2.0 * 32.0 * it32 * (double)threads * blocks;
     if (ms > 0) best32 = fl32 / (ms * 1e-3) / 1e12 > best32 ? fl32 / (ms * 1e-3) / 1e12 : best32;
+    cudaEventRecord(a, ctx->stream);
+    fma2_peak_kernel<<<blocks, threads, 0, ctx->stream>>>(o32, it32 / 2, 0.9999999f, 1e-9f);
+    cudaEventRecord(b, ctx->stream);
+    cudaEventSynchronize(b);
+    cudaEventElapsedTime(&ms, a, b);
+    const double fl2 = 2.0 * 2.0 * 32.0 * (it32 / 2) * (double)threads * blocks;
+    if (ms > 0) best2 = fl2 / (ms * 1e-3) / 1e12 > best2 ? fl2 / (ms * 1e-3) / 1e12 : best2;
   }
   cudaEventDestroy(a);
   cudaEventDestroy(b);
-  FMM_TRY(ctx->check_launch("fma_peak_kernel", 6));
+  FMM_TRY(ctx->check_launch("fma_peak_kernel", 9));
   if (fp64_tflops) *fp64_tflops = best64;
   if (fp32_tflops) *fp32_tflops = best32;
+  if (fp32x2_tflops) *fp32x2_tflops = best2;
   return FMMB200_OK;
 }
 

@@ -33,8 +33,8 @@ int compute_pavg_stretch(Ctx *ctx, const double *d_mom_aos, int64_t N, double *d
 int build_tree(Ctx *ctx, const double *d_pos_aos, int64_t N, int64_t N0, const double *d_consts);
 // Particle records in tree order ("prec64": x,y,z,gamma,ux,uy,uz,0) and, for
 // the mixed form, leaf-local FP32 records ("prec32": x,y,z,gamma,ux,uy,uz,0
-// relative to the leaf's box centre) with the low parts of the coordinates
-// ("prec32lo": x,y,z,0).
+// relative to the leaf's box centre) and the P2P source records ("prec32x2":
+// five float4 of duplicated values -x_hi,-y_hi,-z_hi,-x_lo,-y_lo,-z_lo,gamma,ux,uy,uz).
 // leafpos (optional): leaf cluster of every tree-order position (explicit trees).
 int gather_particles(Ctx *ctx, const double *d_pos_aos, const double *d_mom_aos, bool mixed,
                      const int *leafpos = nullptr);

@@ -292,7 +292,7 @@ __global__ void gather64_kernel(int N, const uint32_t *__restrict__ perm, const 
 __global__ void gather32_kernel(int ml, int N, const uint32_t *__restrict__ perm,
                                 const double *__restrict__ pos, const double *__restrict__ mom,
                                 const double *__restrict__ bbox, const int *__restrict__ leafpos,
-                                float *__restrict__ rec, float *__restrict__ rec_lo) {
+                                float *__restrict__ rec, float4 *__restrict__ rec_x2) {
   int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= N) return;
   int lo, hi;
@@ -307,10 +307,18 @@ __global__ void gather32_kernel(int ml, int N, const uint32_t *__restrict__ perm
   float4 *r = reinterpret_cast<float4 *>(rec + 8 * (int64_t)j);
   r[0] = make_float4(hx, hy, hz, (float)g);
   r[1] = make_float4((float)ux, (float)uy, (float)uz, 0.0f);
-  // hi + lo reproduces the local coordinate to ~2^-48 relative: P2P forms the
-  // difference of two nearby particles exactly from the hi parts (Sterbenz)
-  reinterpret_cast<float4 *>(rec_lo)[j] = make_float4((float)(lx - (double)hx), (float)(ly - (double)hy),
-                                                  (float)(lz - (double)hz), 0.0f);
+  // The P2P source record: hi + lo parts of the local coordinates (hi + lo
+  // reproduces the coordinate to ~2^-48 relative, and P2P forms the difference of
+  // two nearby particles exactly from the hi parts, Sterbenz), negated, then
+  // gamma and u; every value duplicated for packed FP32x2 arithmetic.
+  const float nlx = -(float)(lx - (double)hx), nly = -(float)(ly - (double)hy), nlz = -(float)(lz - (double)hz);
+  const float gf = (float)g, uxf = (float)ux, uyf = (float)uy, uzf = (float)uz;
+  float4 *x2 = rec_x2 + 5 * (int64_t)j;
+  x2[0] = make_float4(-hx, -hx, -hy, -hy);
+  x2[1] = make_float4(-hz, -hz, nlx, nlx);
+  x2[2] = make_float4(nly, nly, nlz, nlz);
+  x2[3] = make_float4(gf, gf, uxf, uxf);
+  x2[4] = make_float4(uyf, uyf, uzf, uzf);
 }
 
 // nodes[c][d][i] = a + (cos(pi*i/n) + 1)/2 * (b - a)  (barylg.jl:25-27, 0-based i)
@@ -511,11 +519,12 @@ int gather_particles(Ctx *ctx, const double *d_pos, const double *d_mom, bool mi
   gather64_kernel<<<ceil_div(N, TB), TB, 0, ctx->stream>>>(N, ctx->get<uint32_t>("perm"), d_pos, d_mom, rec);
   FMM_TRY(ctx->check_launch("gather64_kernel"));
   if (mixed) {
-    float *r32, *lo32;
+    float *r32;
+    float4 *x2;
     FMM_TRY(ctx->ensure("prec32", 8 * (int64_t)N, &r32));
-    FMM_TRY(ctx->ensure("prec32lo", 4 * (int64_t)N, &lo32));
+    FMM_TRY(ctx->ensure("prec32x2", 5 * (int64_t)N, &x2));
     gather32_kernel<<<ceil_div(N, TB), TB, 0, ctx->stream>>>(ctx->ml, N, ctx->get<uint32_t>("perm"), d_pos, d_mom,
-                                                              ctx->get<double>("bbox"), leafpos, r32, lo32);
+                                                              ctx->get<double>("bbox"), leafpos, r32, x2);
     FMM_TRY(ctx->check_launch("gather32_kernel"));
   }
   return FMMB200_OK;

@@ -207,9 +207,11 @@ int fmmb200_direct_device(fmmb200_ctx *ctx, int64_t npar, const double *d_positi
 int fmmb200_direct_noalloc(int64_t npar, const double *d_positions, const double *d_momenta,
                            double charge, double lambda, int64_t ntarget, const int64_t *d_targets,
                            double *d_efields, double *d_bfields, void *stream);
-/* Measured CUDA-core FMA throughput (TFLOP/s, 2 flops per FMA) of the device:
- * the roofline denominators of the M2L / P2P kernels. */
-int fmmb200_measure_fma_peak(fmmb200_ctx *ctx, double *fp64_tflops, double *fp32_tflops);
+/* Measured CUDA-core FMA throughput (TFLOP/s, 2 flops per FMA) of the device with
+ * scalar FP64, scalar FP32 and packed FP32x2 (FFMA2) chains: the roofline
+ * denominators of the M2L / P2P kernels. */
+int fmmb200_measure_fma_peak(fmmb200_ctx *ctx, double *fp64_tflops, double *fp32_tflops,
+                             double *fp32x2_tflops);
 
 #ifdef __cplusplus
 }
