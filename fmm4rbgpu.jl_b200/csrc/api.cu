@@ -425,6 +425,12 @@ int fmmb200_set_timing(fmmb200_ctx *ctx, int enable) {
   return FMMB200_OK;
 }
 
+int fmmb200_set_m2l_engine(fmmb200_ctx *ctx, int engine) {
+  if (!ctx || engine < FMMB200_M2L_AUTO || engine > FMMB200_M2L_TENSOR_CORES) return FMMB200_ERR_INVALID_ARGUMENT;
+  ctx->m2l_engine = engine;
+  return FMMB200_OK;
+}
+
 int fmmb200_debug_fail_alloc(fmmb200_ctx *ctx, int64_t k) {
   if (!ctx || k < 0) return FMMB200_ERR_INVALID_ARGUMENT;
   ctx->fail_alloc_countdown = k;

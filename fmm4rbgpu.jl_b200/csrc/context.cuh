@@ -45,6 +45,7 @@ struct fmmb200_ctx {
   double pavg[3] = {0, 0, 0}, stretch[3] = {1, 1, 1};
   int traversal_steps = 0;
   int list_bits = 1;  // pair keys are (target << list_bits) | source
+  int m2l_engine = 0;  // FMMB200_M2L_*: mixed-form M2L engine
   fmmb200_stats stats{};
 
   // pairwise-summation plan for p_avg (depends on N only)

@@ -21,9 +21,26 @@
 // instructions, two target nodes per thread in the two lanes of a float2; the
 // node offsets are formed in FP64 and rounded, and per-source partial sums are
 // folded into Kahan-compensated FP32 accumulators.
+//
+// Mixed form on the tensor cores (m2l_tc_kernel, degree n <= 4, eta <= 1/2; an
+// opt-in engine -- at n = 4 it measures ~110 ms against ~99 ms for the packed
+// CUDA-core kernel on 2^24 particles: the per-chunk hand-off between the four
+// evaluating warps and the MMA issuer costs more than the 10 FMAs per
+// evaluation it removes, and rsqrt throughput bounds both): per source the
+// M2L is a (target nodes) x (source nodes) kernel matrix K times the 10 packed
+// per-source-node columns V below, so the 10 accumulations per evaluation run
+// as tcgen05 TF32 MMAs.  Each thread owns one target node = one TMEM lane: it
+// evaluates its row of K (3 FP32 ops for the denominator, rsqrt, 2 for s^3) in
+// chunks of 16 source nodes, splits every value into TF32 hi + lo and stores
+// both into a TMEM A buffer (three in rotation); one thread issues the MMAs
+// D += [K_hi; K_lo] x [V_hi | V_lo] (M = 128, N = 32, K = 8) against V held in
+// shared memory.  After each source D is read back (tcgen05.ld), its four
+// hi/lo products are summed and E = x'G - Q, B = W x x' - V is folded into
+// Kahan-compensated FP32 accumulators as in the CUDA-core form.
 #include "device_util.cuh"
 #include "kernels.cuh"
 #include "packed.cuh"
+#include "tcgen05.cuh"
 
 namespace fmmb200 {
 
@@ -200,6 +217,9 @@ __global__ void __launch_bounds__(M2LShape<NDEG>::BT)
 //   (G,G, Gx',Gx') (Gy',Gy', Gz',Gz') (M0,M0, M1,M1) (M2,M2, C0,C0) (C1,C1, C2,C2)
 // with C = M x x', so that one evaluation pair costs 3 packed ops for the
 // denominator, 2 rsqrt, 2 packed ops for s^3, 10 FFMA2 and 5 shared loads.
+// MASK (eta > 1/2, coincident nodes admissible): the factored sums x'G - Q would
+// cancel catastrophically for nodes much closer than the box size, so E and B
+// are accumulated directly (s^3 Gamma R, s^3 M x R) from (G,G,M0,M0) (M1,M1,M2,M2).
 template <int NDEG>
 struct M2LShape2 {
   static constexpr int M = NDEG + 1;
@@ -209,7 +229,7 @@ struct M2LShape2 {
   static constexpr int TPP = (NP + 511) / 512;        // pairs per thread
   static constexpr int BT = (((NP + TPP - 1) / TPP) + 31) / 32 * 32;
   static constexpr int REC = 4 * NN * 4 + NS * 8;     // raw FP32 moments then node coordinates
-  static constexpr int SMEM = 2 * REC + 5 * NN * 16;  // double buffer + packed node data
+  static constexpr int SMEM = 2 * REC + 5 * NN * 16;  // double buffer + packed node data (MASK uses 2/5)
 };
 
 template <int NDEG, bool MASK>
@@ -274,13 +294,19 @@ __global__ void __launch_bounds__(M2LShape2<NDEG>::BT)
           const int bi = b % M, bj = (b / M) % M, bk = b / (M * M);
           const float xb = (float)(SN[bi] - cx), yb = (float)(SN[M + bj] - cy), zb = (float)(SN[2 * M + bk] - cz);
           const float g = G[b], m0 = G[NN + b], m1 = G[2 * NN + b], m2 = G[3 * NN + b];
-          const float c0 = m1 * zb - m2 * yb, c1 = m2 * xb - m0 * zb, c2 = m0 * yb - m1 * xb;
-          float4 *o = pk + 5 * b;
-          o[0] = make_float4(g, g, g * xb, g * xb);
-          o[1] = make_float4(g * yb, g * yb, g * zb, g * zb);
-          o[2] = make_float4(m0, m0, m1, m1);
-          o[3] = make_float4(m2, m2, c0, c0);
-          o[4] = make_float4(c1, c1, c2, c2);
+          if constexpr (MASK) {
+            float4 *o = pk + 2 * b;
+            o[0] = make_float4(g, g, m0, m0);
+            o[1] = make_float4(m1, m1, m2, m2);
+          } else {
+            const float c0 = m1 * zb - m2 * yb, c1 = m2 * xb - m0 * zb, c2 = m0 * yb - m1 * xb;
+            float4 *o = pk + 5 * b;
+            o[0] = make_float4(g, g, g * xb, g * xb);
+            o[1] = make_float4(g * yb, g * yb, g * zb, g * zb);
+            o[2] = make_float4(m0, m0, m1, m1);
+            o[3] = make_float4(m2, m2, c0, c0);
+            o[4] = make_float4(c1, c1, c2, c2);
+          }
         }
       }
       __syncthreads();
@@ -294,25 +320,32 @@ __global__ void __launch_bounds__(M2LShape2<NDEG>::BT)
             const double tx0 = tn[a0 % M] - cx, ty0 = tn[M + (a0 / M) % M] - cy, tz0 = tn[2 * M + a0 / (M * M)] - cz;
             const double tx1 = tn[a1 % M] - cx, ty1 = tn[M + (a1 / M) % M] - cy, tz1 = tn[2 * M + a1 / (M * M)] - cz;
             float2 prx[M], rx2[M], ryv[M];
+            float2 rxv[MASK ? M : 1], nrxv[MASK ? M : 1];
 #pragma unroll
             for (int b = 0; b < M; ++b) {
               const float2 rx = make_float2((float)(tx0 - s_sn[b]), (float)(tx1 - s_sn[b]));
               prx[b] = mul2(px, rx);
               rx2[b] = mul2(rx, rx);
               ryv[b] = make_float2((float)(ty0 - s_sn[M + b]), (float)(ty1 - s_sn[M + b]));
+              if constexpr (MASK) {
+                rxv[b] = rx;
+                nrxv[b] = make_float2(-rx.x, -rx.y);
+              }
             }
+            // factored: (G, Q, W, V) sums; masked: E and B accumulated directly
             float2 g0 = make_float2(0.f, 0.f), q0 = g0, q1 = g0, q2 = g0, w0 = g0, w1 = g0, w2 = g0, v0 = g0,
                    v1 = g0, v2 = g0;
 #pragma unroll 1
             for (int bk = 0; bk < M; ++bk) {
               const float2 rz = make_float2((float)(tz0 - s_sn[2 * M + bk]), (float)(tz1 - s_sn[2 * M + bk]));
+              const float2 nrz = make_float2(-rz.x, -rz.y);
               const float2 prz = mul2(pz, rz);
               const float2 rzz = fma2(rz, rz, eps);
 #pragma unroll
               for (int bj = 0; bj < M; ++bj) {
-                const float2 P = fma2(py, ryv[bj], prz);
-                const float2 A = fma2(ryv[bj], ryv[bj], rzz);
-                const float4 *pb = pk + 5 * M * (bj + M * bk);
+                const float2 ry = ryv[bj], nry = make_float2(-ry.x, -ry.y);
+                const float2 P = fma2(py, ry, prz);
+                const float2 A = fma2(ry, ry, rzz);
 #pragma unroll
                 for (int bi = 0; bi < M; ++bi) {
                   const float2 tt = add2(P, prx[bi]);
@@ -322,32 +355,53 @@ __global__ void __launch_bounds__(M2LShape2<NDEG>::BT)
                   if constexpr (MASK) {
                     s3.x = d.x > (float)kEps64 ? s3.x : 0.f;
                     s3.y = d.y > (float)kEps64 ? s3.y : 0.f;
+                    const float4 *pb = pk + 2 * (bi + M * (bj + M * bk));
+                    const float4 e0 = pb[0], e1 = pb[1];
+                    const float2 gs = mul2(s3, lo2(e0));
+                    const float2 hx = mul2(s3, hi2(e0)), hy = mul2(s3, lo2(e1)), hz = mul2(s3, hi2(e1));
+                    g0 = fma2(gs, rxv[bi], g0);  // E
+                    q0 = fma2(gs, ry, q0);
+                    q1 = fma2(gs, rz, q1);
+                    w0 = fma2(hz, nry, fma2(hy, rz, w0));  // B = s3 M x R
+                    w1 = fma2(hx, nrz, fma2(hz, rxv[bi], w1));
+                    w2 = fma2(hy, nrxv[bi], fma2(hx, ry, w2));
+                  } else {
+                    const float4 *pb = pk + 5 * (bi + M * (bj + M * bk));
+                    const float4 e0 = pb[0], e1 = pb[1], e2 = pb[2], e3 = pb[3], e4 = pb[4];
+                    g0 = fma2(s3, lo2(e0), g0);
+                    q0 = fma2(s3, hi2(e0), q0);
+                    q1 = fma2(s3, lo2(e1), q1);
+                    q2 = fma2(s3, hi2(e1), q2);
+                    w0 = fma2(s3, lo2(e2), w0);
+                    w1 = fma2(s3, hi2(e2), w1);
+                    w2 = fma2(s3, lo2(e3), w2);
+                    v0 = fma2(s3, hi2(e3), v0);
+                    v1 = fma2(s3, lo2(e4), v1);
+                    v2 = fma2(s3, hi2(e4), v2);
                   }
-                  const float4 e0 = pb[5 * bi], e1 = pb[5 * bi + 1], e2 = pb[5 * bi + 2], e3 = pb[5 * bi + 3],
-                               e4 = pb[5 * bi + 4];
-                  g0 = fma2(s3, lo2(e0), g0);
-                  q0 = fma2(s3, hi2(e0), q0);
-                  q1 = fma2(s3, lo2(e1), q1);
-                  q2 = fma2(s3, hi2(e1), q2);
-                  w0 = fma2(s3, lo2(e2), w0);
-                  w1 = fma2(s3, hi2(e2), w1);
-                  w2 = fma2(s3, lo2(e3), w2);
-                  v0 = fma2(s3, hi2(e3), v0);
-                  v1 = fma2(s3, lo2(e4), v1);
-                  v2 = fma2(s3, hi2(e4), v2);
                 }
               }
             }
-            // this source's E and B at both nodes: E = x' G - Q, B = W x x' - V, folded per
-            // source into the compensated sums
-            const float2 xa = make_float2((float)tx0, (float)tx1), ya = make_float2((float)ty0, (float)ty1),
-                         za = make_float2((float)tz0, (float)tz1);
-            kahan_add2(ks[q][0], kc[q][0], sub2(mul2(xa, g0), q0));
-            kahan_add2(ks[q][1], kc[q][1], sub2(mul2(ya, g0), q1));
-            kahan_add2(ks[q][2], kc[q][2], sub2(mul2(za, g0), q2));
-            kahan_add2(ks[q][3], kc[q][3], sub2(sub2(mul2(w1, za), mul2(w2, ya)), v0));
-            kahan_add2(ks[q][4], kc[q][4], sub2(sub2(mul2(w2, xa), mul2(w0, za)), v1));
-            kahan_add2(ks[q][5], kc[q][5], sub2(sub2(mul2(w0, ya), mul2(w1, xa)), v2));
+            if constexpr (MASK) {
+              // coincident nodes are admissible: the factored form would cancel catastrophically
+              kahan_add2(ks[q][0], kc[q][0], g0);
+              kahan_add2(ks[q][1], kc[q][1], q0);
+              kahan_add2(ks[q][2], kc[q][2], q1);
+              kahan_add2(ks[q][3], kc[q][3], w0);
+              kahan_add2(ks[q][4], kc[q][4], w1);
+              kahan_add2(ks[q][5], kc[q][5], w2);
+            } else {
+              // this source's E and B at both nodes: E = x' G - Q, B = W x x' - V, folded per
+              // source into the compensated sums
+              const float2 xa = make_float2((float)tx0, (float)tx1), ya = make_float2((float)ty0, (float)ty1),
+                           za = make_float2((float)tz0, (float)tz1);
+              kahan_add2(ks[q][0], kc[q][0], sub2(mul2(xa, g0), q0));
+              kahan_add2(ks[q][1], kc[q][1], sub2(mul2(ya, g0), q1));
+              kahan_add2(ks[q][2], kc[q][2], sub2(mul2(za, g0), q2));
+              kahan_add2(ks[q][3], kc[q][3], sub2(sub2(mul2(w1, za), mul2(w2, ya)), v0));
+              kahan_add2(ks[q][4], kc[q][4], sub2(sub2(mul2(w2, xa), mul2(w0, za)), v1));
+              kahan_add2(ks[q][5], kc[q][5], sub2(sub2(mul2(w0, ya), mul2(w1, xa)), v2));
+            }
           }
         }
       }
@@ -374,6 +428,298 @@ __global__ void __launch_bounds__(M2LShape2<NDEG>::BT)
   }
 }
 
+// ---------------------------------------------------------------- tensor-core mixed form
+// The K dimension (source nodes) is ordered by x-rows: row r = bj + M bk holds
+// the M nodes bi = 0..M-1, and a 16-column chunk holds RPC = 16 / M whole rows
+// (column 16 c + M i + bi for row r = RPC c + i; the remaining columns are zero
+// padding).  A thread then forms the y/z part of the denominator once per row.
+template <int NDEG>
+struct M2LShapeTC {
+  static constexpr int M = NDEG + 1;
+  static constexpr int NN = M * M * M;                 // <= 125
+  static constexpr int NS = ((3 * M) + 1) & ~1;
+  static constexpr int CH = 16;                        // K columns per chunk (one tcgen05.st.x16)
+  static constexpr int RPC = CH / M;                   // whole x-rows per chunk
+  static constexpr int NR = M * M;                     // x-rows
+  static constexpr int NCH = (NR + RPC - 1) / RPC;
+  static constexpr int KP = NCH * CH;                  // padded K
+  static constexpr int NBUF = 3;                       // TMEM A buffers in rotation
+  static constexpr int NMMA = 32;                      // D columns: 0..9 V_hi products, 16..25 V_lo
+  static constexpr uint32_t LBO = (NMMA / 8) * 128;    // bytes between 4-element K groups of V
+  static constexpr uint32_t SBO = 128;                 // bytes between 8-row groups of V
+  static constexpr int BBYTES = (KP / 4) * (int)LBO;   // one V operand
+  static constexpr int MOM_BYTES = 4 * NN * 4;
+  static constexpr int REC = MOM_BYTES + NS * 8;       // raw FP32 moments then node coordinates
+  static constexpr int SMEM_USED = 2 * BBYTES + 2 * REC;
+  // at most 4 CTAs per SM, so that 4 x 128 TMEM columns never exceed the SM's 512
+  static constexpr int SMEM = SMEM_USED > 48 * 1024 ? SMEM_USED : 48 * 1024;
+  static constexpr uint32_t TMEM_COLS = 128;           // D [0,32), A buffer b at 32 + 32 b (hi 16, lo 16)
+  __host__ __device__ static constexpr int col(int b) {
+    return CH * ((b / M) / RPC) + M * ((b / M) % RPC) + b % M;
+  }
+};
+
+// Warp roles: warps 0-3 evaluate K (thread = target node = TMEM lane) and
+// arrive on full[b] once their slice of A buffer b is in TMEM; warp 4 waits on
+// full[b], issues the chunk's MMAs and commits them to empty[b], which the
+// evaluating warps wait on before reusing buffer b.  The evaluating warps meet
+// in one named barrier per source (V and the node offsets written); they read
+// a source's D while evaluating the next source's first chunk, which the MMAs
+// overwrite only after every warp has arrived for that chunk.
+constexpr int kTcThreads = 160;
+
+template <int NDEG>
+__global__ void __launch_bounds__(kTcThreads, 4)
+    m2l_tc_kernel(const int *__restrict__ ptr, const int *__restrict__ src, const double *__restrict__ nodes,
+                  const double *__restrict__ bbox, const float *__restrict__ mom, float *__restrict__ loc,
+                  const double *__restrict__ consts, int accumulate, int *__restrict__ status) {
+  using S = M2LShapeTC<NDEG>;
+  constexpr int M = S::M, NN = S::NN, NS = S::NS, CH = S::CH, RPC = S::RPC, NR = S::NR, NCH = S::NCH;
+  constexpr int NBUF = S::NBUF, REC = S::REC, MOM_BYTES = S::MOM_BYTES;
+  constexpr uint32_t LBO = S::LBO, SBO = S::SBO;
+  constexpr uint32_t IDESC = idesc_tf32(128, S::NMMA);
+  constexpr int kEvalBar = 1;  // named barrier of the 128 evaluating threads
+  static_assert(NN <= 128 && RPC >= 1, "one target node per TMEM lane, whole rows per chunk");
+  extern __shared__ __align__(1024) unsigned char smem[];
+  unsigned char *sRaw = smem + 2 * S::BBYTES;  // 2 raw source records (TMA double buffer)
+  __shared__ __align__(8) uint64_t bar_tma[2];
+  __shared__ __align__(8) uint64_t bar_full[NBUF];
+  __shared__ __align__(8) uint64_t bar_empty[NBUF];
+  __shared__ __align__(8) uint64_t bar_drain;
+  __shared__ uint32_t s_tmem;
+  __shared__ float s_sn[2][3 * M];  // source node offsets from the target centre, by source parity
+
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int t = blockIdx.x;
+  const int p0 = ptr[t], np = ptr[t + 1] - p0;
+  const double *tn = nodes + (int64_t)t * NS;
+  const double *tb = bbox + 6 * (int64_t)t;
+  const double cx = 0.5 * (tb[0] + tb[3]), cy = 0.5 * (tb[1] + tb[4]), cz = 0.5 * (tb[2] + tb[5]);
+  const int a = tid < NN ? tid : NN - 1;  // rows past NN repeat a node and are not written
+  const float xa = (float)(tn[a % M] - cx), ya = (float)(tn[M + (a / M) % M] - cy),
+              za = (float)(tn[2 * M + a / (M * M)] - cz);
+
+  float ks[6], kc[6];
+#pragma unroll
+  for (int c = 0; c < 6; ++c) ks[c] = kc[c] = 0.f;
+
+  if (np > 0) {
+    for (int e = tid; e < 2 * S::BBYTES / 16; e += kTcThreads)
+      reinterpret_cast<float4 *>(smem)[e] = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (warp == 0) {
+      tmem_alloc(&s_tmem, S::TMEM_COLS);
+      tmem_relinquish();
+    }
+    auto issue = [&](int k, int rb) {
+      const int s = src[p0 + k];
+      unsigned char *dst = sRaw + rb * REC;
+      mbar_arrive_expect_tx(&bar_tma[rb], REC);
+      bulk_g2s(dst, mom + (int64_t)s * 4 * NN, MOM_BYTES, &bar_tma[rb]);
+      bulk_g2s(dst + MOM_BYTES, nodes + (int64_t)s * NS, NS * 8, &bar_tma[rb]);
+    };
+    int issued = 0;  // TMA copies issued (thread 0)
+    if (tid == 0) {
+      mbar_init(&bar_tma[0], 1);
+      mbar_init(&bar_tma[1], 1);
+      for (int b = 0; b < NBUF; ++b) {
+        mbar_init(&bar_full[b], 4);  // one arrival per evaluating warp
+        mbar_init(&bar_empty[b], 1);
+      }
+      mbar_init(&bar_drain, 1);
+      fence_mbar_init();
+      issue(0, 0);
+      issued = 1;
+      if (np > 1) {
+        issue(1, 1);
+        issued = 2;
+      }
+    }
+    fence_proxy_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tbase = s_tmem;
+
+    if (warp == 4) {
+      // ---------------- MMA issuer
+      if ((tid & 31) == 0) {
+        bool ok = true;
+        int k = 0;
+        for (int i = 0; i < np && ok; ++i) {
+          const unsigned char *sV = smem + (i & 1) * S::BBYTES;
+          for (int c = 0; c < NCH; ++c, ++k) {
+            const int b = k % NBUF;
+            if (!mbar_wait_bounded(&bar_full[b], (uint32_t)((k / NBUF) & 1), status)) {
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+            const uint32_t acol = 32 + 32 * (uint32_t)b;
+#pragma unroll
+            for (int kstep = 0; kstep < CH / 8; ++kstep) {
+              const uint64_t bd = smem_desc_noswizzle(sV + ((CH * c + 8 * kstep) / 4) * LBO, LBO, SBO);
+              mma_tf32_ts(tbase, tbase + acol + 8 * kstep, bd, IDESC, (c > 0 || kstep > 0) ? 1u : 0u);
+              mma_tf32_ts(tbase, tbase + acol + 16 + 8 * kstep, bd, IDESC, 1u);
+            }
+            mma_commit(&bar_empty[b]);
+          }
+        }
+        // every MMA issued has completed before TMEM is released
+        mma_commit(&bar_drain);
+        mbar_wait_bounded(&bar_drain, 0, status);
+      }
+    } else {
+      // ---------------- K evaluation (128 threads)
+      const uint32_t lane = (uint32_t)(32 * warp) << 16;
+      const float px = (float)consts[0], py = (float)consts[1], pz = (float)consts[2];
+      const float eps = (float)kEps64;
+      bool fail = false;  // a bounded wait gave up (uniform after each per-source barrier)
+
+      // D holds one source's sums: D[n] + D[16 + n] = (K_hi + K_lo)(V_hi + V_lo)
+      auto readout = [&](int last_chunk) {
+        if (fail) return;
+        if (!mbar_wait_bounded(&bar_empty[last_chunk % NBUF], (uint32_t)((last_chunk / NBUF) & 1), status)) {
+          fail = true;
+          return;
+        }
+        tc_fence_after();
+        uint32_t d0[16], d1[16];
+        tmem_ld16(tbase + lane, d0);
+        tmem_ld16(tbase + lane + 16, d1);
+        tmem_wait_ld();
+        float sum[10];
+#pragma unroll
+        for (int n = 0; n < 10; ++n) sum[n] = __uint_as_float(d0[n]) + __uint_as_float(d1[n]);
+        const float g0 = sum[0], q0 = sum[1], q1 = sum[2], q2 = sum[3], w0 = sum[4], w1 = sum[5], w2 = sum[6];
+        const float v0 = sum[7], v1 = sum[8], v2 = sum[9];
+        const float part[6] = {xa * g0 - q0, ya * g0 - q1, za * g0 - q2,
+                               (w1 * za - w2 * ya) - v0, (w2 * xa - w0 * za) - v1, (w0 * ya - w1 * xa) - v2};
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+          const float y = part[q] - kc[q];
+          const float tsum = ks[q] + y;
+          kc[q] = (tsum - ks[q]) - y;
+          ks[q] = tsum;
+        }
+      };
+
+      int g = 0;         // chunks evaluated so far (global over sources)
+      int consumed = 0;  // TMA copies waited for
+      for (int i = 0; i < np; ++i) {
+        const int rb = i & 1;
+        unsigned char *sV = smem + rb * S::BBYTES;  // V of source i (source i-1's MMAs may still read the other)
+        float *sn = s_sn[rb];
+        const bool got = !fail && mbar_wait_bounded(&bar_tma[rb], (uint32_t)((i >> 1) & 1), status);
+        ++consumed;
+        fail |= !got;
+        if (got) {
+          const float *G = (const float *)(sRaw + rb * REC);
+          const double *SN = (const double *)(sRaw + rb * REC + MOM_BYTES);
+          if (tid < 3 * M) {
+            const int d = tid / M;
+            sn[tid] = (float)(SN[tid] - (d == 0 ? cx : (d == 1 ? cy : cz)));
+          }
+          // V operand: 10 columns per source node, split into TF32 hi (rows 0..9) and lo (rows 16..25)
+          for (int b = tid; b < NN; b += 128) {
+            const int bi = b % M, bj = (b / M) % M, bk = b / (M * M);
+            const float xb = (float)(SN[bi] - cx), yb = (float)(SN[M + bj] - cy), zb = (float)(SN[2 * M + bk] - cz);
+            const float gm = G[b], m0 = G[NN + b], m1 = G[2 * NN + b], m2 = G[3 * NN + b];
+            const float v[10] = {gm, gm * xb, gm * yb, gm * zb, m0, m1, m2,
+                                 m1 * zb - m2 * yb, m2 * xb - m0 * zb, m0 * yb - m1 * xb};
+            const int k = S::col(b);
+            unsigned char *colp = sV + (k / 4) * LBO + (k % 4) * 4;
+#pragma unroll
+            for (int c = 0; c < 10; ++c) {
+              const float h = tf32_hi(v[c]);
+              *(float *)(colp + (c / 8) * SBO + (c % 8) * 16) = h;
+              *(float *)(colp + ((16 + c) / 8) * SBO + ((16 + c) % 8) * 16) = v[c] - h;
+            }
+          }
+        }
+        fence_proxy_async_smem();
+        // V and the node offsets written, raw buffer rb consumed
+        if (bar_or(kEvalBar, 128, fail)) {
+          fail = true;
+          break;
+        }
+        if (tid == 0 && issued < np) {
+          fence_proxy_async_smem();
+          issue(issued, issued & 1);
+          ++issued;
+        }
+        float prx[M], rx2[M];
+#pragma unroll
+        for (int bi = 0; bi < M; ++bi) {
+          const float rx = xa - sn[bi];
+          prx[bi] = px * rx;
+          rx2[bi] = rx * rx;
+        }
+#pragma unroll
+        for (int c = 0; c < NCH; ++c) {
+          const int bsel = g % NBUF;
+          if (g >= NBUF && !fail) {
+            fail |= !mbar_wait_bounded(&bar_empty[bsel], (uint32_t)(((g / NBUF) - 1) & 1), status);
+            tc_fence_after();
+          }
+          uint32_t kh[CH], kl[CH];
+#pragma unroll
+          for (int j = RPC * M; j < CH; ++j) kh[j] = kl[j] = 0u;
+#pragma unroll
+          for (int ir = 0; ir < RPC; ++ir) {
+            const int r = RPC * c + ir;
+            if (r < NR) {
+              const float ry = ya - sn[M + r % M], rz = za - sn[2 * M + r / M];
+              const float P = fmaf(py, ry, pz * rz);
+              const float A = fmaf(ry, ry, fmaf(rz, rz, eps));
+#pragma unroll
+              for (int bi = 0; bi < M; ++bi) {
+                const float tt = P + prx[bi];
+                const float d = fmaf(tt, tt, A + rx2[bi]);
+                const float sv = rsqrt_approx_f32(d);
+                const float kv = (sv * sv) * sv;
+                const float h = tf32_hi(kv);
+                kh[M * ir + bi] = __float_as_uint(h);
+                kl[M * ir + bi] = __float_as_uint(kv - h);
+              }
+            } else {
+#pragma unroll
+              for (int bi = 0; bi < M; ++bi) kh[M * ir + bi] = kl[M * ir + bi] = 0u;
+            }
+          }
+          // the previous source's D, before this source's first chunk lets the MMAs overwrite it
+          if (c == 0 && i > 0) readout(g - 1);
+          const uint32_t acol = 32 + 32 * (uint32_t)bsel;
+          tmem_st16(tbase + lane + acol, kh);
+          tmem_st16(tbase + lane + acol + 16, kl);
+          tmem_wait_st();
+          tc_fence_before();
+          __syncwarp();
+          if ((tid & 31) == 0) mbar_arrive(&bar_full[bsel]);
+          ++g;
+        }
+      }
+      if (g > 0) readout(g - 1);  // the last source
+      if (tid == 0)
+        for (int k = consumed; k < issued; ++k) mbar_wait_bounded(&bar_tma[k & 1], (uint32_t)((k >> 1) & 1), status);
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+      tc_fence_after();
+      tmem_dealloc(tbase, S::TMEM_COLS);
+    }
+  }
+  if (tid < NN) {
+    float *out = loc + (int64_t)t * 6 * NN;
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+      float o = (float)((double)ks[c] - (double)kc[c]);
+      if (accumulate) o += out[c * NN + tid];
+      out[c * NN + tid] = o;
+    }
+  }
+}
+
 template <int NDEG, bool MASK>
 int launch_m2l_fp64(Ctx *ctx, bool accumulate) {
   using S = M2LShape<NDEG>;
@@ -389,8 +735,25 @@ int launch_m2l_fp64(Ctx *ctx, bool accumulate) {
   return ctx->check_launch("m2l_kernel");
 }
 
+template <int NDEG>
+int launch_m2l_tc(Ctx *ctx, bool accumulate) {
+  using S = M2LShapeTC<NDEG>;
+  auto kern = m2l_tc_kernel<NDEG>;
+  FMM_TRY(opt_in_smem(ctx, kern, S::SMEM));
+  if (ctx->nc > 0)
+    kern<<<(unsigned)ctx->nc, kTcThreads, S::SMEM, ctx->stream>>>(
+        ctx->get<int>("m2l_ptr"), ctx->get<int>("m2l_src"), ctx->get<double>("nodes"), ctx->get<double>("bbox"),
+        ctx->get<float>("mom32"), ctx->get<float>("loc32"), ctx->get<double>("consts"), accumulate ? 1 : 0,
+        ctx->d_status);
+  return ctx->check_launch("m2l_tc_kernel");
+}
+
 template <int NDEG, bool MASK>
 int launch_m2l_mixed(Ctx *ctx, bool accumulate) {
+  if constexpr (NDEG <= 4 && !MASK) {
+    // the tensor-core form is factored (E = x'G - Q): only where nodes cannot coincide
+    if (ctx->m2l_engine == FMMB200_M2L_TENSOR_CORES) return launch_m2l_tc<NDEG>(ctx, accumulate);
+  }
   using S = M2LShape2<NDEG>;
   auto kern = m2l_x2_kernel<NDEG, MASK>;
   FMM_TRY(opt_in_smem(ctx, kern, S::SMEM));

@@ -194,15 +194,44 @@ constexpr int kPtThreads = 256;
 constexpr int kPtItems = 8;
 constexpr int kPtTile = kPtThreads * kPtItems;
 
-__global__ void part_count_kernel(int N, const uint32_t *__restrict__ lists, const uint8_t *__restrict__ flag,
-                                  int ntiles, int *__restrict__ tcount) {
+// Left flags of the three lists in list order (fa[a][j]) and their per-tile
+// counts.  In the list of the node's split axis the flag is j <= mid; the other
+// two look the particle up in `flag` -- the level's only random reads.
+// fa rows are fs bytes apart (fs: N rounded up to a multiple of 8).
+__global__ void part_count_kernel(int l, int N, const uint32_t *__restrict__ lists, const uint8_t *__restrict__ flag,
+                                  const int *__restrict__ split, int ntiles, int *__restrict__ tcount,
+                                  uint8_t *__restrict__ fa, int64_t fs) {
   __shared__ int s_warp[33];
-  int j0 = blockIdx.x * kPtTile + threadIdx.x * kPtItems;
+  const int j0 = blockIdx.x * kPtTile + threadIdx.x * kPtItems;
+  int sp[kPtItems];
+  uint8_t inl[kPtItems];  // j <= mid of its node
+  for (int i = 0; i < kPtItems; ++i) {
+    const int j = j0 + i;
+    sp[i] = -1;
+    inl[i] = 0;
+    if (j < N) {
+      int lo, hi;
+      const int k = descend(j, l, N, &lo, &hi);
+      sp[i] = split[k];
+      inl[i] = j <= ((lo + hi) >> 1) ? 1 : 0;
+    }
+  }
   for (int a = 0; a < 3; ++a) {
     int c = 0;
+    uint8_t f[kPtItems];
     for (int i = 0; i < kPtItems; ++i) {
-      int j = j0 + i;
-      if (j < N) c += flag[lists[(int64_t)a * N + j]];
+      const int j = j0 + i;
+      f[i] = 0;
+      if (j < N) f[i] = sp[i] == a ? inl[i] : flag[lists[(int64_t)a * N + j]];
+      c += f[i];
+    }
+    if (j0 + kPtItems <= N) {  // 8 consecutive bytes, 8-byte aligned (j0 is a multiple of 8)
+      uint64_t w = 0;
+      for (int i = 0; i < kPtItems; ++i) w |= (uint64_t)f[i] << (8 * i);
+      *reinterpret_cast<uint64_t *>(fa + a * fs + j0) = w;
+    } else {
+      for (int i = 0; i < kPtItems; ++i)
+        if (j0 + i < N) fa[a * fs + j0 + i] = f[i];
     }
     int tot;
     block_excl_scan(c, s_warp, &tot);
@@ -211,7 +240,7 @@ __global__ void part_count_kernel(int N, const uint32_t *__restrict__ lists, con
 }
 
 __global__ void part_scatter_kernel(int l, int N, const uint32_t *__restrict__ lists,
-                                    const uint8_t *__restrict__ flag, int ntiles, const int *__restrict__ toff,
+                                    const uint8_t *__restrict__ fa, int64_t fs, int ntiles, const int *__restrict__ toff,
                                     const int *__restrict__ nodebase, uint32_t *__restrict__ next,
                                     int *__restrict__ status) {
   __shared__ int s_warp[33];
@@ -238,7 +267,7 @@ __global__ void part_scatter_kernel(int l, int N, const uint32_t *__restrict__ l
       int j = j0 + i;
       if (j < N) {
         p[i] = lists[(int64_t)a * N + j];
-        f[i] = flag[p[i]];
+        f[i] = fa[a * fs + j];
       } else {
         p[i] = 0;
         f[i] = 0;
@@ -456,6 +485,9 @@ int build_tree(Ctx *ctx, const double *d_pos, int64_t N64, int64_t N0, const dou
   FMM_TRY(ctx->ensure("half", nc, &half));
   FMM_TRY(ctx->ensure("nodebase", nc, &nodebase));
   FMM_TRY(ctx->ensure("flag", N, &flag));
+  uint8_t *fa;
+  const int64_t fs = ((int64_t)N + 7) & ~(int64_t)7;  // 8-byte aligned rows for 8-byte stores
+  FMM_TRY(ctx->ensure("flag3", 3 * fs, &fa));
   const int ntiles = ceil_div(N, kPtTile);
   FMM_TRY(ctx->ensure("tcount", 3 * (int64_t)ntiles, &tcount));
   FMM_TRY(ctx->ensure("toff", 3 * (int64_t)ntiles, &toff));
@@ -481,10 +513,10 @@ int build_tree(Ctx *ctx, const double *d_pos, int64_t N64, int64_t N0, const dou
     if (l == ml) break;
     FMM_TRY(exclusive_scan_i32(ctx, half + (cnt_level - 1), nodebase, cnt_level, nullptr));
     flag_kernel<<<ceil_div(N, TB), TB, 0, ctx->stream>>>(l, N, lists, split, flag);
-    part_count_kernel<<<ntiles, kPtThreads, 0, ctx->stream>>>(N, lists, flag, ntiles, tcount);
+    part_count_kernel<<<ntiles, kPtThreads, 0, ctx->stream>>>(l, N, lists, flag, split, ntiles, tcount, fa, fs);
     FMM_TRY(ctx->check_launch("flag/part_count kernels", 2));
     FMM_TRY(exclusive_scan_i32(ctx, tcount, toff, 3 * (int64_t)ntiles, nullptr));
-    part_scatter_kernel<<<ntiles, kPtThreads, 0, ctx->stream>>>(l, N, lists, flag, ntiles, toff, nodebase, next,
+    part_scatter_kernel<<<ntiles, kPtThreads, 0, ctx->stream>>>(l, N, lists, fa, fs, ntiles, toff, nodebase, next,
                                                                  ctx->d_status);
     FMM_TRY(ctx->check_launch("part_scatter_kernel"));
     uint32_t *t = lists;

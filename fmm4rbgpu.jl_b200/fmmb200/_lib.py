@@ -34,6 +34,10 @@ ERR_CAPACITY = 7
 PRECISION_FP64 = 0
 PRECISION_MIXED = 1
 
+M2L_AUTO = 0
+M2L_CUDA_CORES = 1
+M2L_TENSOR_CORES = 2
+
 
 class FMMB200Error(RuntimeError):
     """A non-zero status from libfmmb200 (the reference raises ErrorException)."""
@@ -100,6 +104,7 @@ SIGNATURES = {
     "fmmb200_direct": (ctypes.c_int, [c_vp, c_i64, p_f64, p_f64, c_f64, c_f64, c_i64, p_i64, p_f64, p_f64]),
     "fmmb200_direct_device": (ctypes.c_int, [c_vp, c_i64, c_vp, c_vp, c_f64, c_f64, c_i64, c_vp, c_vp, c_vp]),
     "fmmb200_measure_fma_peak": (ctypes.c_int, [c_vp, p_f64, p_f64, p_f64]),
+    "fmmb200_set_m2l_engine": (ctypes.c_int, [c_vp, ctypes.c_int]),
     "fmmb200_direct_noalloc": (ctypes.c_int, [c_i64, c_vp, c_vp, c_f64, c_f64, c_i64, c_vp, c_vp, c_vp, c_vp]),
 }
 

@@ -144,6 +144,14 @@ class Context:
     def set_timing(self, enable: bool):
         self._check(self._lib.fmmb200_set_timing(self._h, int(bool(enable))))
 
+    def set_m2l_engine(self, engine: str):
+        """Mixed-form M2L engine: "auto" / "cuda_cores" (packed FP32x2 kernel) or
+        "tensor_cores" (tcgen05 TF32 MMAs for n <= 4 and eta <= 1/2)."""
+        codes = {"auto": L.M2L_AUTO, "cuda_cores": L.M2L_CUDA_CORES, "tensor_cores": L.M2L_TENSOR_CORES}
+        if engine not in codes:
+            raise ValueError(f"engine must be one of {sorted(codes)}")
+        self._check(self._lib.fmmb200_set_m2l_engine(self._h, codes[engine]))
+
     def debug_fail_alloc(self, k: int):
         self._check(self._lib.fmmb200_debug_fail_alloc(self._h, int(k)))
 

@@ -74,6 +74,16 @@ const char *fmmb200_last_error(const fmmb200_ctx *ctx);
 int fmmb200_set_stream(fmmb200_ctx *ctx, void *stream);
 /* Record per-stage CUDA events (stats ms_*); off by default. */
 int fmmb200_set_timing(fmmb200_ctx *ctx, int enable);
+/* Engine of the mixed-form M2L (no counterpart in the reference, whose M2L is one
+ * FP64 kernel).  FMMB200_M2L_AUTO (default) and FMMB200_M2L_CUDA_CORES: the
+ * packed FP32x2 CUDA-core kernel.  FMMB200_M2L_TENSOR_CORES: tcgen05 TF32 MMAs
+ * with hi/lo splitting for n <= 4 and eta <= 1/2 (the CUDA-core kernel
+ * otherwise); same accuracy class, slower at n = 4 on B200.  The FP64 path is
+ * not affected. */
+#define FMMB200_M2L_AUTO 0
+#define FMMB200_M2L_CUDA_CORES 1
+#define FMMB200_M2L_TENSOR_CORES 2
+int fmmb200_set_m2l_engine(fmmb200_ctx *ctx, int engine);
 /* Fault injection for tests: the k-th next device allocation fails (k >= 1; 0 disables). */
 int fmmb200_debug_fail_alloc(fmmb200_ctx *ctx, int64_t k);
 

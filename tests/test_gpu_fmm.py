@@ -57,12 +57,17 @@ def test_config1_against_bruteforce(gpu_ctx, oracle_mod):
     assert np.all(B == 0.0) and np.all(Bb == 0.0)
 
 
-def test_mixed_matches_fp64(gpu_ctx):
+@pytest.mark.parametrize("engine", ["auto", "tensor_cores"])
+def test_mixed_matches_fp64(gpu_ctx, engine):
     import fmmb200
 
     pos, mom = make("gauss", 2**17, 2)
     E, B = gpu_ctx.forward(pos, mom, fmmb200.FMMB200(n=4, N0=125, eta=0.5))
-    Em, Bm = gpu_ctx.forward(pos, mom, fmmb200.FMMB200(n=4, N0=125, eta=0.5, precision="mixed"))
+    try:
+        gpu_ctx.set_m2l_engine(engine)
+        Em, Bm = gpu_ctx.forward(pos, mom, fmmb200.FMMB200(n=4, N0=125, eta=0.5, precision="mixed"))
+    finally:
+        gpu_ctx.set_m2l_engine("auto")
     assert rel(Em, E) < MIXED_TOL and rel(Bm, B) < MIXED_TOL
 
 

@@ -225,6 +225,39 @@ def test_m2l_matches_oracle(gpu_ctx, oracle_mod, n, precision):
     assert rel(e, re) < tol and rel(b, rb) < tol
 
 
+@pytest.mark.parametrize("n", [1, 2, 3, 4])
+@pytest.mark.parametrize("eta", [0.5, 0.7])
+def test_m2l_mixed_engines_agree(gpu_ctx, oracle_mod, n, eta):
+    """Both mixed M2L engines match the oracle within the mixed tolerance: the
+    tensor-core form (tcgen05 TF32 hi/lo MMAs, n <= 4, eta <= 1/2) and the packed
+    FP32x2 CUDA-core kernel.  eta = 0.7 admits coincident nodes: both engines then
+    run the non-factored CUDA-core accumulation."""
+    pos, mom, stretch, t, _ = tree_case(oracle_mod, N=4000, N0=30)
+    NN = (n + 1) ** 3
+    nc = t["nc"]
+    rng = np.random.default_rng(10 + n)
+    g = rng.random(NN * nc)
+    m = rng.normal(0, 1, 3 * NN * nc) + np.tile([0.0, 0.0, 50.0], NN * nc)
+    _, m2l = oracle_mod.interaction_lists(t["children"], t["bboxes"], stretch, eta)
+    m2l = oracle_mod.sort_by_target(m2l)
+    pavg = np.array([0.01, -0.02, 50.0])
+    re, rb = np.zeros(3 * NN * nc), np.zeros(3 * NN * nc)
+    oracle_mod.m2l(oracle_mod.VARIANT_GPU, n, t["bboxes"], g, m, m2l, pavg, re, rb)
+    got = {}
+    try:
+        for engine in ("tensor_cores", "cuda_cores"):
+            gpu_ctx.set_m2l_engine(engine)
+            e, b = np.zeros(3 * NN * nc), np.zeros(3 * NN * nc)
+            gpu_ctx.m2l(n, t["bboxes"], g, m, m2l, pavg, e, b, precision="mixed")
+            assert np.all(np.isfinite(e)) and np.all(np.isfinite(b))
+            assert rel(e, re) < MIXED_STAGE_TOL and rel(b, rb) < MIXED_STAGE_TOL, engine
+            got[engine] = (e, b)
+    finally:
+        gpu_ctx.set_m2l_engine("auto")
+    if eta > 0.5:  # same kernel either way
+        assert np.array_equal(got["tensor_cores"][0], got["cuda_cores"][0])
+
+
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_p2p_far_field_reference_case(gpu_ctx, precision):
     # test/test_gpu_fmm/test_gpu_interaction.jl:50-96
