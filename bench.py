@@ -10,6 +10,8 @@ tree build, traversal, P2M/M2M, M2L, P2P, L2L/L2P.
   fp64     the plain FP64 path on the same inputs
   e2e      the mixed form through the host-pointer C-ABI (the call the drop-in
            makes): pinned host inputs copied in and fields copied out every step
+  fwd_bwd  one forward (saving its state) plus the hand-written adjoint of
+           L = sum(w.E + v.B) back to positions and momenta, device-resident
   roofline the dominant kernel (M2L) against the measured CUDA-core FMA peak
   accuracy rel-L2 of mixed vs FP64 over all particles, and of both vs an FP64
            direct sum (GPU) on 4096 seeded targets
@@ -61,6 +63,10 @@ def parse():
     ap.add_argument("--ref-sample", type=int, default=2**18, help="particles per reference-arm step")
     ap.add_argument("--skip-cpu-baseline", action="store_true")
     ap.add_argument("--skip-e2e", action="store_true")
+    ap.add_argument("--skip-backward", action="store_true")
+    ap.add_argument("--m2l-engine", choices=["auto", "cuda_cores", "tensor_cores"], default="auto",
+                    help="mixed-form M2L engine (fmmb200_set_m2l_engine)")
+    ap.add_argument("--bwd-steps", type=int, default=3, help="timed fwd+bwd steps (after 2 warm-up steps)")
     return ap.parse_args()
 
 
@@ -229,6 +235,7 @@ def run_ours(args, world, rank, local):
     ctx = fmmb200.Context(local)
     ctx.set_stream(stream.cuda_stream)
     ctx.set_timing(True)
+    ctx.set_m2l_engine(args.m2l_engine)
     L = ctx._lib
     alg_mixed = fmmb200.FMMB200(n=args.n, N0=args.N0, eta=args.eta, precision="mixed")
     alg_fp64 = fmmb200.FMMB200(n=args.n, N0=args.N0, eta=args.eta, precision="fp64")
@@ -289,6 +296,38 @@ def run_ours(args, world, rank, local):
            "mixed_vs_direct": {"E": rel(E[tg], Ed), "B": rel(B[tg], Bd)},
            "direct_targets": int(tg.numel())}
 
+    # forward + adjoint (the gradient path of the fields), device-resident
+    fwd_bwd = None
+    if not args.skip_backward:
+        gen = torch.Generator(device=dev).manual_seed(args.seed + 7)
+        gE = torch.randn((N, 3), dtype=torch.float64, device=dev, generator=gen)
+        gB = torch.randn((N, 3), dtype=torch.float64, device=dev, generator=gen)
+        gx = torch.empty_like(gE)
+        gu = torch.empty_like(gE)
+
+        def fb_step(alg, e, b):
+            ctx.forward_device(N, pos.data_ptr(), mom.data_ptr(), e.data_ptr(), b.data_ptr(), alg,
+                               save_for_backward=True)
+            ctx.backward_device(gE.data_ptr(), gB.data_ptr(), gx.data_ptr(), gu.data_ptr())
+
+        fwd_bwd = {}
+        for name, alg, e, b, ms_f in (("mixed", alg_mixed, E, B, ms_mixed), ("fp64", alg_fp64, E64, B64, ms_fp64)):
+            for _ in range(2):
+                fb_step(alg, e, b)
+            stream.synchronize()
+            barrier(world)
+            ev0 = torch.cuda.Event(enable_timing=True)
+            ev1 = torch.cuda.Event(enable_timing=True)
+            ev0.record(stream)
+            for _ in range(args.bwd_steps):
+                fb_step(alg, e, b)
+            ev1.record(stream)
+            ev1.synchronize()
+            ms_fb = max_over_ranks(world, ev0.elapsed_time(ev1) / args.bwd_steps)
+            fwd_bwd[name] = {"ms_per_step": ms_fb, "value": replicas.aggregate_rate(world, N, ms_fb),
+                             "unit": "particles/s", "ratio_to_forward": ms_fb / ms_f, "steps": args.bwd_steps,
+                             "warmup": 2, "grad_finite": bool(torch.isfinite(gx).all() and torch.isfinite(gu).all())}
+
     # roofline of the dominant kernel (M2L) against the measured CUDA-core FMA peak
     p64 = ctypes.c_double()
     p32 = ctypes.c_double()
@@ -297,12 +336,18 @@ def run_ours(args, world, rank, local):
     m2l_flops = 41.0 * st["m2l_kernel_evals"]
     ach32 = m2l_flops / (st["ms_m2l"] * 1e-3) / 1e12 if st["ms_m2l"] > 0 else 0.0
     ach64 = 41.0 * st64["m2l_kernel_evals"] / (st64["ms_m2l"] * 1e-3) / 1e12 if st64["ms_m2l"] > 0 else 0.0
-    roof = {"kernel": "m2l_kernel<4, mixed>", "bound": "fp32", "achieved": ach32, "peak": p32.value,
-            "unit": "TFLOP/s", "frac": ach32 / p32.value if p32.value else None, "traffic": None,
-            "peak_source": "measured FP32 FMA throughput (fmmb200_measure_fma_peak) on this GPU",
+    kname = "m2l_tc_kernel" if (args.m2l_engine == "tensor_cores" and args.n <= 4) else "m2l_x2_kernel"
+    # DRAM bytes of the packed M2L kernel per M2L pair (read + write), from an ncu capture of the
+    # same kernel on the N = 2^22 bunch (1.051e9 B for 2,557,114 pairs), scaled by this run's pairs
+    traffic = 411.1 * st["nm2l"] if kname == "m2l_x2_kernel" and args.n == 4 else None
+    roof = {"kernel": f"{kname}<{args.n}> (mixed)", "bound": "fp32", "achieved": ach32, "peak": p32.value,
+            "unit": "TFLOP/s", "frac": ach32 / p32.value if p32.value else None, "traffic": traffic,
+            "traffic_unit": "bytes per launch (scaled by M2L pairs from the N=2^22 capture)",
+            "peak_source": "measured FP32 FMA throughput of this GPU (fmmb200_measure_fma_peak): the kernel runs "
+                           "on the CUDA cores, so neither the HBM nor the bf16 tensor figure bounds it",
             "peak_fp32x2_measured": p2.value,
             "flops_per_launch": m2l_flops, "ms_per_launch": st["ms_m2l"],
-            "fp64": {"kernel": "m2l_kernel<4, fp64>", "achieved": ach64, "peak": p64.value,
+            "fp64": {"kernel": f"m2l_kernel<{args.n}> (fp64)", "achieved": ach64, "peak": p64.value,
                      "frac": ach64 / p64.value if p64.value else None, "ms_per_launch": st64["ms_m2l"]}}
 
     # end to end through the host-pointer C-ABI (pinned host buffers)
@@ -359,6 +404,7 @@ def run_ours(args, world, rank, local):
                      "ncluster": st["ncluster"], "model_flops_per_step": mf,
                      "model_tflops_mixed": mf / (ms_mixed * 1e-3) / 1e12,
                      "model_tflops_fp64": mf / (ms_fp64 * 1e-3) / 1e12, "device_bytes": st["device_bytes"]},
+            "fwd_bwd": fwd_bwd,
             "roofline": roof,
             "cpu_baseline": cpu,
             "e2e": e2e,

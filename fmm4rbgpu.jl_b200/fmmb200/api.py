@@ -201,6 +201,11 @@ class Context:
         self._check(self._lib.fmmb200_backward(self._h, _pd(ge), _pd(gb), _pd(gx), _pd(gu)))
         return gx, gu
 
+    def backward_device(self, d_grad_e: int, d_grad_b: int, d_grad_pos: int, d_grad_mom: int):
+        """Device-pointer adjoint of the saved forward (asynchronous on the context stream)."""
+        self._check(self._lib.fmmb200_backward_device(self._h, ctypes.c_void_p(d_grad_e), ctypes.c_void_p(d_grad_b),
+                                                      ctypes.c_void_p(d_grad_pos), ctypes.c_void_p(d_grad_mom)))
+
     # ---------------------------------------------------------------- introspection
     def tree_info(self) -> dict:
         info = np.zeros(8, np.int64)
