@@ -20,10 +20,12 @@
 // dL/da += (xi - 1) G, dL/db += -xi G; for a node of the cluster itself:
 // dL/da += (1 - t_i) G_i, dL/db += t_i G_i.
 #include <cmath>
+#include <type_traits>
 
 #include "device_util.cuh"
 #include "interp_util.cuh"
 #include "kernels.cuh"
+#include "packed.cuh"
 
 namespace fmmb200 {
 
@@ -436,7 +438,8 @@ __global__ void __launch_bounds__(BShape<NDEG>::BT)
 //   gx_a     += f c - 3 d^{-5/2} (R.c)(R + (p.R) p),  c = [f1] c1 - [f2] c2
 //   gGamma_a -= [f2] f gE_s[b].R,   gM_a -= [f2] f R x gB_s[b]
 //   gp       += [f1] -3 d^{-5/2} (p.R)(R.c1) R
-template <int NDEG>
+// MASK (eta > 1/2): coincident nodes contribute nothing, as in the forward.
+template <int NDEG, bool MASK>
 __global__ void __launch_bounds__(BShape<NDEG>::BT)
     m2l_bwd_kernel(const int *__restrict__ ptr, const int *__restrict__ src, const uint8_t *__restrict__ flg,
                    const double *__restrict__ nodes, ChebT ct, const double *__restrict__ mom,
@@ -529,7 +532,7 @@ __global__ void __launch_bounds__(BShape<NDEG>::BT)
                 const double rx = rxv[bi];
                 const double pr = P + prx[bi];
                 const double d = pr * pr + (A + rx2[bi]);
-                const double s = rsqrt(d);
+                const double s = MASK && !(d > kEps64) ? 0.0 : rsqrt(d);
                 const double f = s * s * s, f5 = f * s * s;
                 double c0 = 0, c1 = 0, c2 = 0;
                 if (f1) {
@@ -598,6 +601,260 @@ __global__ void __launch_bounds__(BShape<NDEG>::BT)
   double g3[6] = {gp[0], gp[1], gp[2], 0, 0, 0};
   block_sum<6>(g3, s_red);
   if (tid < 3) gp_part[3 * (int64_t)t + tid] = g3[tid];
+}
+
+// ---------------------------------------------------------------- M2L^T, mixed form
+// The adjoint of the mixed forward evaluates M2L^T in FP32: the saved FP32 moments
+// and the local adjoints (rounded from FP64) of every cluster are packed into one
+// record [Gamma | M(3) | gE(3) | gB(3)] x NN, RECF floats per cluster.
+template <int NDEG>
+struct MBShape2 {
+  static constexpr int M = NDEG + 1;
+  static constexpr int NN = M * M * M;
+  static constexpr int NS = ((3 * M) + 1) & ~1;
+  static constexpr int NP = (NN + 1) / 2;           // target-node pairs, one per thread
+  static constexpr int BT = ((NP + 31) / 32) * 32;
+  static constexpr int RECF = ((10 * NN + 3) / 4) * 4;
+  static constexpr int RAWB = RECF * 4;              // bytes of the FP32 part of a staged record
+  static constexpr int REC = RAWB + NS * 8;          // ... followed by the node coordinates
+  static constexpr int NACC = 13;                    // per target: axf(3) axw(3) ap(3) aG aM(3)
+  static constexpr int SMEM = 2 * REC + 5 * NN * 16 + 2 * NACC * BT * 8;
+};
+
+template <int NDEG>
+__global__ void adj_rec32_kernel(int64_t nc, const float *__restrict__ mom32, const double *__restrict__ gloc,
+                                 float *__restrict__ rec) {
+  using S = MBShape2<NDEG>;
+  constexpr int NN = S::NN, RECF = S::RECF;
+  const int64_t total = nc * RECF;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t c = i / RECF;
+    const int e = (int)(i - c * RECF);
+    float v = 0.f;
+    if (e < 4 * NN)
+      v = mom32[c * 4 * NN + e];
+    else if (e < 10 * NN)
+      v = (float)gloc[c * 6 * NN + (e - 4 * NN)];
+    rec[i] = v;
+  }
+}
+
+// Per target cluster over its union list, two target nodes per thread in the two
+// lanes of packed FP32x2 instructions; the quantities are those of m2l_bwd_kernel:
+//   c = [f1] (Gamma_b gE_a + gB_a x M_b) - [f2] (Gamma_a gE_b + gB_b x M_a)
+//   gx_a += f c - 3 f5 (R.c)(R + (p.R) p)            (accumulated as axf - 3 axw)
+//   gp   += [f1] -3 f5 (p.R)(R.c1) R                  (accumulated as -3 ap)
+//   gGamma_a -= [f2] f gE_b.R,  gM_a -= [f2] f R x gB_b
+// Per source the FP32 partial sums are added into per-thread FP64 sums in shared memory.
+template <int NDEG, bool MASK>
+__global__ void __launch_bounds__(MBShape2<NDEG>::BT)
+    m2l_bwd_x2_kernel(const int *__restrict__ ptr, const int *__restrict__ src, const uint8_t *__restrict__ flg,
+                      const double *__restrict__ nodes, const double *__restrict__ bbox, ChebT ct,
+                      const float *__restrict__ rec32, const double *__restrict__ consts, double *__restrict__ gmom,
+                      double *__restrict__ gbox, double *__restrict__ gp_part, int *__restrict__ status) {
+  using S = MBShape2<NDEG>;
+  constexpr int M = S::M, NN = S::NN, NS = S::NS, NP = S::NP, BT = S::BT, RECF = S::RECF, RAWB = S::RAWB;
+  constexpr int REC = S::REC, NACC = S::NACC;
+  extern __shared__ __align__(16) unsigned char smem[];
+  float4 *pk = (float4 *)(smem + 2 * REC);                     // 5 NN duplicated per-node operands
+  double *s_acc = (double *)(smem + 2 * REC + 5 * NN * 16);     // [2 NACC][BT] FP64 sums
+  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ double s_sn[3 * M];  // source node offsets from the target centre
+  __shared__ double s_red[32 * 6];
+
+  const int tid = threadIdx.x;
+  const int t = blockIdx.x;
+  const int p0 = ptr[t], np = ptr[t + 1] - p0;
+  const double *tn = nodes + (int64_t)t * NS;
+  const double *tb = bbox + 6 * (int64_t)t;
+  const double cx = 0.5 * (tb[0] + tb[3]), cy = 0.5 * (tb[1] + tb[4]), cz = 0.5 * (tb[2] + tb[5]);
+  const bool act = tid < NP;
+  const bool two = act && tid + NP < NN;  // the second lane holds a real node
+  const int a0 = act ? tid : 0, a1 = two ? tid + NP : a0;
+  const double tx0 = tn[a0 % M] - cx, ty0 = tn[M + (a0 / M) % M] - cy, tz0 = tn[2 * M + a0 / (M * M)] - cz;
+  const double tx1 = tn[a1 % M] - cx, ty1 = tn[M + (a1 / M) % M] - cy, tz1 = tn[2 * M + a1 / (M * M)] - cz;
+  const float *own = rec32 + (int64_t)t * RECF;
+  auto pair = [&](int q) { return make_float2(own[q * NN + a0], own[q * NN + a1]); };
+  const float2 Ga = pair(0), Ma0 = pair(1), Ma1 = pair(2), Ma2 = pair(3);
+  const float2 gE0 = pair(4), gE1 = pair(5), gE2 = pair(6), gB0 = pair(7), gB1 = pair(8), gB2 = pair(9);
+  const float2 nGa = make_float2(-Ga.x, -Ga.y), nMa0 = make_float2(-Ma0.x, -Ma0.y),
+               nMa1 = make_float2(-Ma1.x, -Ma1.y), nMa2 = make_float2(-Ma2.x, -Ma2.y);
+  const float2 ngB0 = make_float2(-gB0.x, -gB0.y), ngB1 = make_float2(-gB1.x, -gB1.y),
+               ngB2 = make_float2(-gB2.x, -gB2.y);
+  for (int q = 0; q < 2 * NACC; ++q) s_acc[q * BT + tid] = 0.0;
+  const float2 px = dup2((float)consts[0]), py = dup2((float)consts[1]), pz = dup2((float)consts[2]);
+  const float2 eps = dup2((float)kEps64);
+  const float epsf = (float)kEps64;
+
+  if (np > 0) {
+    if (tid == 0) {
+      mbar_init(&bar[0], 1);
+      mbar_init(&bar[1], 1);
+      fence_mbar_init();
+    }
+    __syncthreads();
+    auto issue = [&](int k, int bb) {
+      const int s = src[p0 + k];
+      unsigned char *dst = smem + bb * REC;
+      mbar_arrive_expect_tx(&bar[bb], REC);
+      bulk_g2s(dst, rec32 + (int64_t)s * RECF, RAWB, &bar[bb]);
+      bulk_g2s(dst + RAWB, nodes + (int64_t)s * NS, NS * 8, &bar[bb]);
+    };
+    if (tid == 0) issue(0, 0);
+    for (int i = 0; i < np; ++i) {
+      const int bb = i & 1;
+      const int fl = flg[p0 + i];
+      if (tid == 0 && i + 1 < np) {
+        fence_proxy_async_smem();
+        issue(i + 1, bb ^ 1);
+      }
+      const bool ok = mbar_wait_bounded(&bar[bb], (uint32_t)((i >> 1) & 1), status);
+      const float *G = (const float *)(smem + bb * REC);
+      const double *SN = (const double *)(smem + bb * REC + RAWB);
+      if (ok) {
+        for (int e = tid; e < 3 * M; e += BT) {
+          const int d = e / M;
+          s_sn[e] = SN[e] - (d == 0 ? cx : (d == 1 ? cy : cz));
+        }
+        for (int b = tid; b < NN; b += BT) {
+          float v[10];
+#pragma unroll
+          for (int q = 0; q < 10; ++q) v[q] = G[q * NN + b];
+          float4 *o = pk + 5 * b;
+          o[0] = make_float4(v[0], v[0], v[1], v[1]);  // Gamma, M0
+          o[1] = make_float4(v[2], v[2], v[3], v[3]);  // M1, M2
+          o[2] = make_float4(v[4], v[4], v[5], v[5]);  // gE0, gE1
+          o[3] = make_float4(v[6], v[6], v[7], v[7]);  // gE2, gB0
+          o[4] = make_float4(v[8], v[8], v[9], v[9]);  // gB1, gB2
+        }
+      }
+      __syncthreads();
+      if (ok && act) {
+        float2 rxv[M], nrxv[M], prx[M], rx2[M], ryv[M];
+#pragma unroll
+        for (int b = 0; b < M; ++b) {
+          const float2 rx = make_float2((float)(tx0 - s_sn[b]), (float)(tx1 - s_sn[b]));
+          rxv[b] = rx;
+          nrxv[b] = make_float2(-rx.x, -rx.y);
+          prx[b] = mul2(px, rx);
+          rx2[b] = mul2(rx, rx);
+          ryv[b] = make_float2((float)(ty0 - s_sn[M + b]), (float)(ty1 - s_sn[M + b]));
+        }
+        const float2 z = make_float2(0.f, 0.f);
+        float2 axf0 = z, axf1 = z, axf2 = z, axw0 = z, axw1 = z, axw2 = z, ap0 = z, ap1 = z, ap2 = z;
+        float2 aG = z, aM0 = z, aM1 = z, aM2 = z;
+        auto sweep = [&](auto FL) {
+          constexpr int F = decltype(FL)::value;
+#pragma unroll 1
+          for (int bk = 0; bk < M; ++bk) {
+            const float2 rz = make_float2((float)(tz0 - s_sn[2 * M + bk]), (float)(tz1 - s_sn[2 * M + bk]));
+            const float2 nrz = make_float2(-rz.x, -rz.y);
+            const float2 prz = mul2(pz, rz);
+            const float2 rzz = fma2(rz, rz, eps);
+#pragma unroll
+            for (int bj = 0; bj < M; ++bj) {
+              const float2 ry = ryv[bj], nry = make_float2(-ry.x, -ry.y);
+              const float2 P = fma2(py, ry, prz);
+              const float2 A = fma2(ry, ry, rzz);
+              const float4 *pb = pk + 5 * M * (bj + M * bk);
+#pragma unroll
+              for (int bi = 0; bi < M; ++bi) {
+                const float2 rx = rxv[bi];
+                const float2 tt = add2(P, prx[bi]);  // p.R
+                const float2 d = fma2(tt, tt, add2(A, rx2[bi]));
+                float2 sv = rsqrt2(d);
+                if constexpr (MASK) {
+                  sv.x = d.x > epsf ? sv.x : 0.f;
+                  sv.y = d.y > epsf ? sv.y : 0.f;
+                }
+                const float2 s2 = mul2(sv, sv);
+                const float2 f = mul2(s2, sv), f5 = mul2(f, s2);
+                float2 c0 = z, c1 = z, c2 = z, rc = z;
+                if constexpr ((F & 1) != 0) {
+                  const float4 q0 = pb[5 * bi], q1 = pb[5 * bi + 1];
+                  const float2 Gb = lo2(q0), Mb0 = hi2(q0), Mb1 = lo2(q1), Mb2 = hi2(q1);
+                  c0 = fma2(Gb, gE0, fma2(gB1, Mb2, mul2(ngB2, Mb1)));
+                  c1 = fma2(Gb, gE1, fma2(gB2, Mb0, mul2(ngB0, Mb2)));
+                  c2 = fma2(Gb, gE2, fma2(gB0, Mb1, mul2(ngB1, Mb0)));
+                  rc = fma2(rz, c2, fma2(ry, c1, mul2(rx, c0)));
+                  const float2 w1 = mul2(mul2(f5, tt), rc);
+                  ap0 = fma2(w1, rx, ap0);
+                  ap1 = fma2(w1, ry, ap1);
+                  ap2 = fma2(w1, rz, ap2);
+                }
+                if constexpr ((F & 2) != 0) {
+                  const float4 q2 = pb[5 * bi + 2], q3 = pb[5 * bi + 3], q4 = pb[5 * bi + 4];
+                  const float2 E0 = lo2(q2), E1 = hi2(q2), E2 = lo2(q3), H0 = hi2(q3), H1 = lo2(q4), H2 = hi2(q4);
+                  const float2 d0 = fma2(nGa, E0, fma2(Ma1, H2, mul2(nMa2, H1)));
+                  const float2 d1 = fma2(nGa, E1, fma2(Ma2, H0, mul2(nMa0, H2)));
+                  const float2 d2 = fma2(nGa, E2, fma2(Ma0, H1, mul2(nMa1, H0)));
+                  c0 = add2(c0, d0);
+                  c1 = add2(c1, d1);
+                  c2 = add2(c2, d2);
+                  rc = fma2(rz, d2, fma2(ry, d1, fma2(rx, d0, rc)));
+                  const float2 er = fma2(rz, E2, fma2(ry, E1, mul2(rx, E0)));
+                  aG = fma2(f, er, aG);
+                  aM0 = fma2(f, fma2(ry, H2, mul2(nrz, H1)), aM0);
+                  aM1 = fma2(f, fma2(rz, H0, mul2(nrxv[bi], H2)), aM1);
+                  aM2 = fma2(f, fma2(rx, H1, mul2(nry, H0)), aM2);
+                }
+                const float2 fr = mul2(f5, rc);
+                axf0 = fma2(f, c0, axf0);
+                axf1 = fma2(f, c1, axf1);
+                axf2 = fma2(f, c2, axf2);
+                axw0 = fma2(fr, fma2(tt, px, rx), axw0);
+                axw1 = fma2(fr, fma2(tt, py, ry), axw1);
+                axw2 = fma2(fr, fma2(tt, pz, rz), axw2);
+              }
+            }
+          }
+        };
+        if (fl == 3)
+          sweep(std::integral_constant<int, 3>{});
+        else if (fl == 1)
+          sweep(std::integral_constant<int, 1>{});
+        else if (fl == 2)
+          sweep(std::integral_constant<int, 2>{});
+        const float2 part[NACC] = {axf0, axf1, axf2, axw0, axw1, axw2, ap0, ap1, ap2, aG, aM0, aM1, aM2};
+#pragma unroll
+        for (int q = 0; q < NACC; ++q) {
+          s_acc[(2 * q) * BT + tid] += (double)part[q].x;
+          s_acc[(2 * q + 1) * BT + tid] += (double)part[q].y;
+        }
+      }
+      __syncthreads();  // the packed data and buffer bb are rewritten later
+    }
+  }
+  // moment adjoints (source role), the box from the node-position gradients, d/dp_avg
+  double gbx[6] = {0, 0, 0, 0, 0, 0};
+  double gpv[6] = {0, 0, 0, 0, 0, 0};
+  if (act) {
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      if (u == 1 && !two) break;
+      const int a = u == 0 ? a0 : a1;
+      double v[NACC];
+#pragma unroll
+      for (int q = 0; q < NACC; ++q) v[q] = s_acc[(2 * q + u) * BT + tid];
+      double *gm = gmom + (int64_t)t * 4 * NN;
+      gm[a] -= v[9];
+      gm[NN + a] -= v[10];
+      gm[2 * NN + a] -= v[11];
+      gm[3 * NN + a] -= v[12];
+      const int idx[3] = {a % M, (a / M) % M, a / (M * M)};
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        const double gx = v[d] - 3.0 * v[3 + d];
+        gbx[d] += (1.0 - ct.t[idx[d]]) * gx;
+        gbx[3 + d] += ct.t[idx[d]] * gx;
+        gpv[d] += -3.0 * v[6 + d];
+      }
+    }
+  }
+  block_sum<6>(gbx, s_red);
+  if (tid < 6) gbox[6 * (int64_t)t + tid] += gbx[tid];
+  block_sum<6>(gpv, s_red);
+  if (tid < 3) gp_part[3 * (int64_t)t + tid] = gpv[tid];
 }
 
 // ---------------------------------------------------------------- P2P^T (per target leaf)
@@ -727,6 +984,208 @@ __global__ void __launch_bounds__(128)
   }
 }
 
+// ---------------------------------------------------------------- P2P^T, mixed form
+// Source records of the mixed adjoint (8 float4, every value duplicated): the
+// forward's P2P record (negated hi/lo leaf-local coordinates, gamma, u) followed
+// by the particle's field adjoint a_E, a_B.
+__global__ void adj_p2p_rec_kernel(int N, const float4 *__restrict__ prec32x2, const double *__restrict__ adj,
+                                   float4 *__restrict__ rec) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= N) return;
+  float4 *o = rec + 8 * (int64_t)p;
+#pragma unroll
+  for (int q = 0; q < 5; ++q) o[q] = prec32x2[5 * (int64_t)p + q];
+  float a[6];
+#pragma unroll
+  for (int q = 0; q < 6; ++q) a[q] = (float)adj[(int64_t)q * N + p];
+  o[5] = make_float4(a[0], a[0], a[1], a[1]);
+  o[6] = make_float4(a[2], a[2], a[3], a[3]);
+  o[7] = make_float4(a[4], a[4], a[5], a[5]);
+}
+
+// Per target leaf over its union list, G lanes per pair of target particles, the
+// two targets in the two lanes of packed FP32x2 instructions (quantities as in
+// p2p_bwd_kernel).  R = x_p - x_j is formed in the source leaf's frame from hi + lo
+// parts as in the mixed forward; R = 0 (the particle itself, or a duplicate
+// position) contributes nothing, as in the forward.  Per tile the FP32 partial sums
+// are added into FP64 registers.
+template <int G>
+__global__ void __launch_bounds__(128)
+    p2p_bwd_x2_kernel(int leaf0, const int *__restrict__ lohi, const int *__restrict__ ptr,
+                      const int *__restrict__ src, const uint8_t *__restrict__ flg, const double *__restrict__ bbox,
+                      const float4 *__restrict__ recb, const double *__restrict__ rec16, int N,
+                      double *__restrict__ gxu, int *__restrict__ status) {
+  constexpr int REC = 8;  // float4 per source record
+  __shared__ __align__(16) float4 buf[2][kPbTile * REC];
+  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ int s_cnt[2], s_flag[2];
+  __shared__ double s_centre[2][3];
+  __shared__ int s_warp[33];
+  const int tid = threadIdx.x, TG = blockDim.x / G, tl = tid / G, g = tid % G;
+  const int c = leaf0 + blockIdx.x;
+  const int tlo = lohi[2 * c], thi = lohi[2 * c + 1], tcnt = thi - tlo + 1;
+  const int p0 = ptr[c], np = ptr[c + 1] - p0;
+  int w = 0;
+  for (int k = tid; k < np; k += blockDim.x) {
+    const int s = src[p0 + k];
+    w += (lohi[2 * s + 1] - lohi[2 * s] + kPbTile) / kPbTile;
+  }
+  int W;
+  block_excl_scan(w, s_warp, &W);
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  int wk = 0, woff = 0;
+  auto issue = [&](int bb) {
+    const int s = src[p0 + wk];
+    const int slo = lohi[2 * s], scnt = lohi[2 * s + 1] - slo + 1;
+    const int cnt = scnt - woff < kPbTile ? scnt - woff : kPbTile;
+    s_cnt[bb] = cnt;
+    s_flag[bb] = flg[p0 + wk];
+    const double *sb = bbox + 6 * (int64_t)s;
+    s_centre[bb][0] = 0.5 * (sb[0] + sb[3]);
+    s_centre[bb][1] = 0.5 * (sb[1] + sb[4]);
+    s_centre[bb][2] = 0.5 * (sb[2] + sb[5]);
+    const uint32_t bytes = (uint32_t)(cnt * REC * sizeof(float4));
+    mbar_arrive_expect_tx(&bar[bb], bytes);
+    bulk_g2s(&buf[bb][0], recb + (int64_t)(slo + woff) * REC, bytes, &bar[bb]);
+    woff += kPbTile;
+    if (woff >= scnt) {
+      woff = 0;
+      ++wk;
+    }
+  };
+  const float2 z = make_float2(0.f, 0.f), eps = dup2((float)kEps64), three = dup2(3.f);
+  int it = 0;
+  for (int tc = 0; tc < tcnt; tc += 2 * TG) {
+    const int ti0 = tc + tl, ti1 = tc + tl + TG;
+    const bool act0 = ti0 < tcnt, act1 = ti1 < tcnt;
+    const int64_t pj0 = tlo + (act0 ? ti0 : 0), pj1 = tlo + (act1 ? ti1 : 0);
+    const double *r0 = rec16 + 16 * pj0, *r1 = rec16 + 16 * pj1;
+    const double X0 = r0[0], Y0 = r0[1], Z0 = r0[2], X1 = r1[0], Y1 = r1[1], Z1 = r1[2];
+    auto pr = [&](int q) { return make_float2((float)r0[q], (float)r1[q]); };
+    const float2 gp = pr(3), up0 = pr(4), up1 = pr(5), up2 = pr(6);
+    const float2 aE0 = pr(8), aE1 = pr(9), aE2 = pr(10), aB0 = pr(11), aB1 = pr(12), aB2 = pr(13);
+    const float2 nup0 = make_float2(-up0.x, -up0.y), nup1 = make_float2(-up1.x, -up1.y),
+                 nup2 = make_float2(-up2.x, -up2.y);
+    const float2 naB0 = make_float2(-aB0.x, -aB0.y), naB1 = make_float2(-aB1.x, -aB1.y),
+                 naB2 = make_float2(-aB2.x, -aB2.y);
+    const float2 igp = make_float2(1.f / gp.x, 1.f / gp.y);
+    double acc0[6] = {0, 0, 0, 0, 0, 0}, acc1[6] = {0, 0, 0, 0, 0, 0};  // gx(3), gu(3)
+    if (tid == 0) {
+      wk = 0;
+      woff = 0;
+      if (W > 0) {
+        fence_proxy_async_smem();
+        issue(it & 1);
+      }
+    }
+    for (int i = 0; i < W; ++i, ++it) {
+      const int bb = it & 1;
+      if (tid == 0 && i + 1 < W) {
+        fence_proxy_async_smem();
+        issue(bb ^ 1);
+      }
+      const bool ok = mbar_wait_bounded(&bar[bb], (uint32_t)((it >> 1) & 1), status);
+      if (ok && act0) {
+        const int cnt = s_cnt[bb], fl = s_flag[bb];
+        const double scx = s_centre[bb][0], scy = s_centre[bb][1], scz = s_centre[bb][2];
+        const double dx0 = X0 - scx, dy0 = Y0 - scy, dz0 = Z0 - scz, dx1 = X1 - scx, dy1 = Y1 - scy, dz1 = Z1 - scz;
+        const float2 xh = make_float2((float)dx0, (float)dx1), yh = make_float2((float)dy0, (float)dy1),
+                     zh = make_float2((float)dz0, (float)dz1);
+        const float2 xl = make_float2((float)(dx0 - (double)xh.x), (float)(dx1 - (double)xh.y));
+        const float2 yl = make_float2((float)(dy0 - (double)yh.x), (float)(dy1 - (double)yh.y));
+        const float2 zl = make_float2((float)(dz0 - (double)zh.x), (float)(dz1 - (double)zh.y));
+        float2 gx0 = z, gx1 = z, gx2 = z, gu0 = z, gu1 = z, gu2 = z;
+        const float4 *S = &buf[bb][0];
+        auto sweep = [&](auto FL) {
+          constexpr int F = decltype(FL)::value;
+#pragma unroll 2
+          for (int j = g; j < cnt; j += G) {
+            const float4 *q = S + j * REC;
+            const float4 q0 = q[0], q1 = q[1], q2 = q[2];
+            const float2 rx = add2(add2(xh, lo2(q0)), add2(xl, hi2(q1)));
+            const float2 ry = add2(add2(yh, hi2(q0)), add2(yl, lo2(q2)));
+            const float2 rz = add2(add2(zh, lo2(q1)), add2(zl, hi2(q2)));
+            const float2 rr = fma2(rx, rx, fma2(ry, ry, mul2(rz, rz)));
+            if constexpr ((F & 1) != 0) {  // j's field at the target: uses u_j, gamma_j and the target's a_E, a_B
+              const float4 q3 = q[3], q4 = q[4];
+              const float2 gj = lo2(q3), uj0 = hi2(q3), uj1 = lo2(q4), uj2 = hi2(q4);
+              const float2 ur = fma2(uj2, rz, fma2(uj1, ry, mul2(uj0, rx)));
+              const float2 d = fma2(ur, ur, add2(rr, eps));
+              float2 sv = rsqrt2(d);
+              sv.x = rr.x > 0.f ? sv.x : 0.f;
+              sv.y = rr.y > 0.f ? sv.y : 0.f;
+              const float2 s2 = mul2(sv, sv), f = mul2(s2, sv);
+              const float2 k0 = fma2(gj, aE0, fma2(aB1, uj2, mul2(naB2, uj1)));
+              const float2 k1 = fma2(gj, aE1, fma2(aB2, uj0, mul2(naB0, uj2)));
+              const float2 k2 = fma2(gj, aE2, fma2(aB0, uj1, mul2(naB1, uj0)));
+              const float2 rk = fma2(rz, k2, fma2(ry, k1, mul2(rx, k0)));
+              const float2 nw = mul2(mul2(f, mul2(s2, rk)), dup2(-3.f));  // -3 f5 (R.k), no FP32 overflow
+              gx0 = fma2(nw, fma2(ur, uj0, rx), fma2(f, k0, gx0));
+              gx1 = fma2(nw, fma2(ur, uj1, ry), fma2(f, k1, gx1));
+              gx2 = fma2(nw, fma2(ur, uj2, rz), fma2(f, k2, gx2));
+            }
+            if constexpr ((F & 2) != 0) {  // the target's field at j: uses u_p, gamma_p and j's a_E, a_B
+              const float4 q5 = q[5], q6 = q[6], q7 = q[7];
+              const float2 e0 = lo2(q5), e1 = hi2(q5), e2 = lo2(q6), h0 = hi2(q6), h1 = lo2(q7), h2 = hi2(q7);
+              const float2 ur = fma2(up2, rz, fma2(up1, ry, mul2(up0, rx)));
+              const float2 d = fma2(ur, ur, add2(rr, eps));
+              float2 sv = rsqrt2(d);
+              sv.x = rr.x > 0.f ? sv.x : 0.f;
+              sv.y = rr.y > 0.f ? sv.y : 0.f;
+              const float2 s2 = mul2(sv, sv), f = mul2(s2, sv), nf = make_float2(-f.x, -f.y);
+              const float2 k0 = fma2(gp, e0, fma2(h1, up2, mul2(h2, nup1)));
+              const float2 k1 = fma2(gp, e1, fma2(h2, up0, mul2(h0, nup2)));
+              const float2 k2 = fma2(gp, e2, fma2(h0, up1, mul2(h1, nup0)));
+              const float2 rk = fma2(rz, k2, fma2(ry, k1, mul2(rx, k0)));
+              const float2 w = mul2(mul2(f, mul2(s2, rk)), three);  // 3 f5 (R.k)
+              gx0 = fma2(w, fma2(ur, up0, rx), fma2(nf, k0, gx0));
+              gx1 = fma2(w, fma2(ur, up1, ry), fma2(nf, k1, gx1));
+              gx2 = fma2(w, fma2(ur, up2, rz), fma2(nf, k2, gx2));
+              const float2 wu = mul2(w, ur);
+              const float2 er = mul2(mul2(fma2(rz, e2, fma2(ry, e1, mul2(rx, e0))), nf), igp);
+              gu0 = fma2(nf, sub2(mul2(ry, h2), mul2(rz, h1)), fma2(er, up0, fma2(wu, rx, gu0)));
+              gu1 = fma2(nf, sub2(mul2(rz, h0), mul2(rx, h2)), fma2(er, up1, fma2(wu, ry, gu1)));
+              gu2 = fma2(nf, sub2(mul2(rx, h1), mul2(ry, h0)), fma2(er, up2, fma2(wu, rz, gu2)));
+            }
+          }
+        };
+        if (fl == 3)
+          sweep(std::integral_constant<int, 3>{});
+        else if (fl == 1)
+          sweep(std::integral_constant<int, 1>{});
+        else if (fl == 2)
+          sweep(std::integral_constant<int, 2>{});
+        const float2 part[6] = {gx0, gx1, gx2, gu0, gu1, gu2};
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+          acc0[q] += (double)part[q].x;
+          acc1[q] += (double)part[q].y;
+        }
+      }
+      __syncthreads();  // buffer bb is refilled two iterations later
+    }
+#pragma unroll
+    for (int q = 0; q < 6; ++q)
+#pragma unroll
+      for (int o = 1; o < G; o <<= 1) {
+        acc0[q] += __shfl_xor_sync(0xffffffffu, acc0[q], o);
+        acc1[q] += __shfl_xor_sync(0xffffffffu, acc1[q], o);
+      }
+    if (g == 0) {
+#pragma unroll
+      for (int q = 0; q < 6; ++q) {
+        if (act0) gxu[(int64_t)q * N + pj0] += acc0[q];
+        if (act1) gxu[(int64_t)q * N + pj1] += acc1[q];
+      }
+    }
+  }
+}
+
 // ---------------------------------------------------------------- boxes, p_avg, scatter
 // A box side of cluster c is attained by argext[c]: pass its adjoint to the child
 // holding that particle (levels top-down).
@@ -836,9 +1295,22 @@ int run_backward_t(Ctx *ctx, const double *d_ge, const double *d_gb, double *d_g
       FMM_TRY(ctx->check_launch("transfer_bwd_kernel<L2L>"));
     }
   }
-  // M2L^T over the union lists
-  {
-    auto k = m2l_bwd_kernel<NDEG>;
+  // M2L^T over the union lists (coincident nodes are possible only for eta > 1/2)
+  const bool mask = !(ctx->eta <= 0.5);
+  if (ctx->precision == FMMB200_PRECISION_MIXED) {
+    using S2 = MBShape2<NDEG>;
+    float *rec32;
+    FMM_TRY(ctx->ensure("bwd_rec32", (int64_t)S2::RECF * nc, &rec32));
+    adj_rec32_kernel<NDEG><<<592, 256, 0, st>>>(nc, ctx->get<float>("mom32"), gloc, rec32);
+    FMM_TRY(ctx->check_launch("adj_rec32_kernel"));
+    auto k = mask ? m2l_bwd_x2_kernel<NDEG, true> : m2l_bwd_x2_kernel<NDEG, false>;
+    FMM_TRY(opt_in_smem(ctx, k, S2::SMEM));
+    k<<<(unsigned)nc, S2::BT, S2::SMEM, st>>>(ctx->get<int>("m2lu_ptr"), ctx->get<int>("m2lu_src"),
+                                              ctx->get<uint8_t>("m2lu_flag"), nodes, bbox, ct, rec32,
+                                              ctx->get<double>("consts"), gmom, gbox, gpp, ctx->d_status);
+    FMM_TRY(ctx->check_launch("m2l_bwd_x2_kernel"));
+  } else {
+    auto k = mask ? m2l_bwd_kernel<NDEG, true> : m2l_bwd_kernel<NDEG, false>;
     const int sm = 2 * (10 * NN + NS) * 8;
     FMM_TRY(opt_in_smem(ctx, k, sm));
     k<<<(unsigned)nc, S::BT, sm, st>>>(ctx->get<int>("m2lu_ptr"), ctx->get<int>("m2lu_src"),
@@ -865,7 +1337,28 @@ int run_backward_t(Ctx *ctx, const double *d_ge, const double *d_gb, double *d_g
     FMM_TRY(ctx->check_launch("leaf_bwd_kernel<P2M>"));
   }
   // P2P^T (G lanes per target particle as in the forward)
-  {
+  if (ctx->precision == FMMB200_PRECISION_MIXED) {
+    float4 *recb;
+    FMM_TRY(ctx->ensure("bwd_p2p_rec", 8 * (int64_t)N, &recb));
+    adj_p2p_rec_kernel<<<ceil_div(N, 256), 256, 0, st>>>(N, ctx->get<float4>("prec32x2"), adj, recb);
+    FMM_TRY(ctx->check_launch("adj_p2p_rec_kernel"));
+    const int *pp = ctx->get<int>("p2pu_ptr"), *ps = ctx->get<int>("p2pu_src");
+    const uint8_t *pf = ctx->get<uint8_t>("p2pu_flag");
+    // two targets per lane group: G lanes share them (as in the mixed forward)
+    if (ctx->max_leaf <= 32)
+      p2p_bwd_x2_kernel<8><<<(unsigned)nleaf, 128, 0, st>>>((int)ctx->leaf0, lohi, pp, ps, pf, bbox, recb, rec16, N,
+                                                            gxu, ctx->d_status);
+    else if (ctx->max_leaf <= 64)
+      p2p_bwd_x2_kernel<4><<<(unsigned)nleaf, 128, 0, st>>>((int)ctx->leaf0, lohi, pp, ps, pf, bbox, recb, rec16, N,
+                                                            gxu, ctx->d_status);
+    else if (ctx->max_leaf <= 128)
+      p2p_bwd_x2_kernel<2><<<(unsigned)nleaf, 128, 0, st>>>((int)ctx->leaf0, lohi, pp, ps, pf, bbox, recb, rec16, N,
+                                                            gxu, ctx->d_status);
+    else
+      p2p_bwd_x2_kernel<1><<<(unsigned)nleaf, 128, 0, st>>>((int)ctx->leaf0, lohi, pp, ps, pf, bbox, recb, rec16, N,
+                                                            gxu, ctx->d_status);
+    FMM_TRY(ctx->check_launch("p2p_bwd_x2_kernel"));
+  } else {
     const int *pp = ctx->get<int>("p2pu_ptr"), *ps = ctx->get<int>("p2pu_src");
     const uint8_t *pf = ctx->get<uint8_t>("p2pu_flag");
     if (ctx->max_leaf <= 32)

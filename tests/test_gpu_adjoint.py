@@ -117,6 +117,50 @@ def test_mixed_forward_adjoint_matches_fp64(gpu_ctx):
     assert rel(gxm, gx) < 1e-4 and rel(gum, gu) < 1e-4
 
 
+@pytest.mark.parametrize("kind,N,n,N0,eta", [("gauss", 30000, 4, 125, 0.5), ("gauss", 30000, 4, 32, 0.5),
+                                              ("uniform", 20000, 3, 100, 0.5), ("beamlets", 20000, 2, 200, 0.5),
+                                              ("gauss", 20000, 4, 64, 0.7)])
+def test_mixed_adjoint_kernels_match_fp64(gpu_ctx, kind, N, n, N0, eta):
+    """The mixed form's adjoint runs M2L^T and P2P^T in packed FP32 (hi/lo
+    coordinates in the near field); it stays within 1e-4 of the FP64 adjoint for
+    every lane-group width (leaf sizes 32..256) and for eta > 1/2 (masked nodes)."""
+    import fmmb200
+    from fmmb200 import beams
+
+    gen = {"gauss": beams.gaussian_bunch, "uniform": beams.uniform, "beamlets": beams.beamlets}[kind]
+    pos, mom = gen(N, seed=4)
+    if kind == "uniform":
+        mom = np.random.default_rng(5).normal(0, 0.5, (N, 3))  # nonzero momenta: B and d/du are exercised
+    rng = np.random.default_rng(2)
+    w = rng.normal(size=(N, 3))
+    v = rng.normal(size=(N, 3))
+    _, gx, gu = fmm_loss_grad(gpu_ctx, pos, mom, fmmb200.FMMB200(n=n, N0=N0, eta=eta), w, v)
+    _, gxm, gum = fmm_loss_grad(gpu_ctx, pos, mom, fmmb200.FMMB200(n=n, N0=N0, eta=eta, precision="mixed"), w, v)
+    assert np.all(np.isfinite(gxm)) and np.all(np.isfinite(gum))
+    assert rel(gxm, gx) < 1e-4 and rel(gum, gu) < 1e-4, (rel(gxm, gx), rel(gum, gu))
+
+
+def test_mixed_single_leaf_matches_autograd_direct_sum(gpu_ctx):
+    import fmmb200
+    from fmmb200 import beams
+
+    N = 200
+    pos, mom = beams.gaussian_bunch(N, seed=11)
+    rng = np.random.default_rng(3)
+    w = rng.normal(size=(N, 3))
+    v = rng.normal(size=(N, 3))
+    _, gx, gu = fmm_loss_grad(gpu_ctx, pos, mom, fmmb200.FMMB200(n=4, N0=256, eta=0.5, precision="mixed"), w, v)
+    _, gxt, gut = direct_grad_torch(pos, mom, w, v)
+    assert rel(gx, gxt) < 1e-5 and rel(gu, gut) < 1e-5
+
+
+def test_gradient_matches_finite_differences_eta_above_half(gpu_ctx):
+    import fmmb200
+
+    fd, an = _fd_case(gpu_ctx, fmmb200.FMMB200(n=3, N0=40, eta=0.7), 4096)
+    assert rel(an, fd) < 1e-4, (rel(an, fd), np.c_[fd, an][:8])
+
+
 def test_gradient_close_to_autograd_direct_sum(gpu_ctx):
     import fmmb200
     from fmmb200 import beams
