@@ -62,7 +62,10 @@ __device__ __forceinline__ void block_sum(double (&v)[V], double *s_red /* [32][
 
 // ---------------------------------------------------------------- gather / init
 // adj: a = amp * (dL/dE, dL/dB) in tree order (SoA); rec16: the particle record
-// (x,y,z,gamma,ux,uy,uz,0) followed by (aE, aB, 0, 0) -- 128 bytes per particle.
+// (x,y,z,gamma,ux,uy,uz,0) followed by (aE, aB, 0, 0) and two doubles of padding --
+// kRecB = 18 doubles (144 bytes) per particle, so that the records that the lanes
+// of a warp read at once in P2P^T fall on distinct shared-memory banks.
+constexpr int kRecB = 18;
 __global__ void adj_gather_kernel(int N, const uint32_t *__restrict__ perm, const double *__restrict__ ge,
                                   const double *__restrict__ gb, double amp, const double *__restrict__ prec,
                                   double *__restrict__ adj, double *__restrict__ rec16, double *__restrict__ gxu) {
@@ -74,15 +77,14 @@ __global__ void adj_gather_kernel(int N, const uint32_t *__restrict__ perm, cons
     v[q] = amp * ge[o + q];
     v[3 + q] = amp * gb[o + q];
   }
-  double *r = rec16 + 16 * (int64_t)p;
+  double *r = rec16 + kRecB * (int64_t)p;
   for (int q = 0; q < 8; ++q) r[q] = prec[8 * (int64_t)p + q];
   for (int q = 0; q < 6; ++q) {
     adj[(int64_t)q * N + p] = v[q];
     r[8 + q] = v[q];
     gxu[(int64_t)q * N + p] = 0.0;
   }
-  r[14] = 0.0;
-  r[15] = 0.0;
+  for (int q = 14; q < kRecB; ++q) r[q] = 0.0;
 }
 
 // ---------------------------------------------------------------- L2P^T / P2M^T (per leaf)
@@ -716,10 +718,13 @@ __global__ void __launch_bounds__(MBShape2<NDEG>::BT)
           const int d = e / M;
           s_sn[e] = SN[e] - (d == 0 ? cx : (d == 1 ? cy : cz));
         }
+        // A pair in only one role zeroes the other role's half of the source data:
+        // that role's terms then vanish exactly, so one evaluation loop serves all pairs.
+        const float k1 = (fl & 1) ? 1.f : 0.f, k2 = (fl & 2) ? 1.f : 0.f;
         for (int b = tid; b < NN; b += BT) {
           float v[10];
 #pragma unroll
-          for (int q = 0; q < 10; ++q) v[q] = G[q * NN + b];
+          for (int q = 0; q < 10; ++q) v[q] = G[q * NN + b] * (q < 4 ? k1 : k2);
           float4 *o = pk + 5 * b;
           o[0] = make_float4(v[0], v[0], v[1], v[1]);  // Gamma, M0
           o[1] = make_float4(v[2], v[2], v[3], v[3]);  // M1, M2
@@ -809,12 +814,7 @@ __global__ void __launch_bounds__(MBShape2<NDEG>::BT)
             }
           }
         };
-        if (fl == 3)
-          sweep(std::integral_constant<int, 3>{});
-        else if (fl == 1)
-          sweep(std::integral_constant<int, 1>{});
-        else if (fl == 2)
-          sweep(std::integral_constant<int, 2>{});
+        if (fl != 0) sweep(std::integral_constant<int, 3>{});
         const float2 part[NACC] = {axf0, axf1, axf2, axw0, axw1, axw2, ap0, ap1, ap2, aG, aM0, aM1, aM2};
 #pragma unroll
         for (int q = 0; q < NACC; ++q) {
@@ -871,7 +871,7 @@ __global__ void __launch_bounds__(128)
     p2p_bwd_kernel(int leaf0, const int *__restrict__ lohi, const int *__restrict__ ptr, const int *__restrict__ src,
                    const uint8_t *__restrict__ flg, const double *__restrict__ rec16, int N,
                    double *__restrict__ gxu, int *__restrict__ status) {
-  __shared__ __align__(16) double buf[2][kPbTile * 16];
+  __shared__ __align__(16) double buf[2][kPbTile * kRecB];
   __shared__ __align__(8) uint64_t bar[2];
   __shared__ int meta[2][3];  // cnt, flag, first tree index
   __shared__ int s_warp[33];
@@ -900,8 +900,8 @@ __global__ void __launch_bounds__(128)
     meta[bb][0] = cnt;
     meta[bb][1] = flg[p0 + wk];
     meta[bb][2] = slo + woff;
-    mbar_arrive_expect_tx(&bar[bb], (uint32_t)(cnt * 128));
-    bulk_g2s(&buf[bb][0], rec16 + 16 * (int64_t)(slo + woff), (uint32_t)(cnt * 128), &bar[bb]);
+    mbar_arrive_expect_tx(&bar[bb], (uint32_t)(cnt * kRecB * 8));
+    bulk_g2s(&buf[bb][0], rec16 + kRecB * (int64_t)(slo + woff), (uint32_t)(cnt * kRecB * 8), &bar[bb]);
     woff += kPbTile;
     if (woff >= scnt) {
       woff = 0;
@@ -913,7 +913,7 @@ __global__ void __launch_bounds__(128)
     const int ti = tc + tl;
     const bool active = ti < tcnt;
     const int pi = tlo + (active ? ti : 0);
-    const double *rp = rec16 + 16 * (int64_t)pi;
+    const double *rp = rec16 + kRecB * (int64_t)pi;
     const double xp = rp[0], yp = rp[1], zp = rp[2], gp_ = rp[3], up0 = rp[4], up1 = rp[5], up2 = rp[6];
     const double aE0 = rp[8], aE1 = rp[9], aE2 = rp[10], aB0 = rp[11], aB1 = rp[12], aB2 = rp[13];
     double acc[6] = {0, 0, 0, 0, 0, 0};  // gx(3), gu(3)
@@ -936,7 +936,7 @@ __global__ void __launch_bounds__(128)
         const int cnt = meta[bb][0], fl = meta[bb][1], first = meta[bb][2];
         for (int j = g; j < cnt; j += G) {
           if (first + j == pi) continue;
-          const double *r = &buf[bb][16 * j];
+          const double *r = &buf[bb][kRecB * j];
           const double rx = xp - r[0], ry = yp - r[1], rz = zp - r[2];
           const double rr = rx * rx + ry * ry + rz * rz;
           if (fl & 1) {
@@ -985,14 +985,16 @@ __global__ void __launch_bounds__(128)
 }
 
 // ---------------------------------------------------------------- P2P^T, mixed form
-// Source records of the mixed adjoint (8 float4, every value duplicated): the
-// forward's P2P record (negated hi/lo leaf-local coordinates, gamma, u) followed
-// by the particle's field adjoint a_E, a_B.
+// Source records of the mixed adjoint (9 float4, every value duplicated): the
+// forward's P2P record (negated hi/lo leaf-local coordinates, gamma, u), the
+// particle's field adjoint a_E, a_B and one float4 of padding -- a 144-byte stride
+// puts the records that the lane groups of a warp read at once on distinct
+// shared-memory banks (a 128-byte stride maps them all to the same four).
 __global__ void adj_p2p_rec_kernel(int N, const float4 *__restrict__ prec32x2, const double *__restrict__ adj,
                                    float4 *__restrict__ rec) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= N) return;
-  float4 *o = rec + 8 * (int64_t)p;
+  float4 *o = rec + 9 * (int64_t)p;
 #pragma unroll
   for (int q = 0; q < 5; ++q) o[q] = prec32x2[5 * (int64_t)p + q];
   float a[6];
@@ -1001,6 +1003,7 @@ __global__ void adj_p2p_rec_kernel(int N, const float4 *__restrict__ prec32x2, c
   o[5] = make_float4(a[0], a[0], a[1], a[1]);
   o[6] = make_float4(a[2], a[2], a[3], a[3]);
   o[7] = make_float4(a[4], a[4], a[5], a[5]);
+  o[8] = make_float4(0.f, 0.f, 0.f, 0.f);
 }
 
 // Per target leaf over its union list, G lanes per pair of target particles, the
@@ -1015,12 +1018,13 @@ __global__ void __launch_bounds__(128)
                       const int *__restrict__ src, const uint8_t *__restrict__ flg, const double *__restrict__ bbox,
                       const float4 *__restrict__ recb, const double *__restrict__ rec16, int N,
                       double *__restrict__ gxu, int *__restrict__ status) {
-  constexpr int REC = 8;  // float4 per source record
+  constexpr int REC = 9;  // float4 per source record (the last one padding)
   __shared__ __align__(16) float4 buf[2][kPbTile * REC];
   __shared__ __align__(8) uint64_t bar[2];
   __shared__ int s_cnt[2], s_flag[2];
   __shared__ double s_centre[2][3];
   __shared__ int s_warp[33];
+  __shared__ double s_acc[12][128];  // per thread: gx(3), gu(3) of both targets, FP64
   const int tid = threadIdx.x, TG = blockDim.x / G, tl = tid / G, g = tid % G;
   const int c = leaf0 + blockIdx.x;
   const int tlo = lohi[2 * c], thi = lohi[2 * c + 1], tcnt = thi - tlo + 1;
@@ -1064,8 +1068,7 @@ __global__ void __launch_bounds__(128)
     const int ti0 = tc + tl, ti1 = tc + tl + TG;
     const bool act0 = ti0 < tcnt, act1 = ti1 < tcnt;
     const int64_t pj0 = tlo + (act0 ? ti0 : 0), pj1 = tlo + (act1 ? ti1 : 0);
-    const double *r0 = rec16 + 16 * pj0, *r1 = rec16 + 16 * pj1;
-    const double X0 = r0[0], Y0 = r0[1], Z0 = r0[2], X1 = r1[0], Y1 = r1[1], Z1 = r1[2];
+    const double *r0 = rec16 + kRecB * pj0, *r1 = rec16 + kRecB * pj1;
     auto pr = [&](int q) { return make_float2((float)r0[q], (float)r1[q]); };
     const float2 gp = pr(3), up0 = pr(4), up1 = pr(5), up2 = pr(6);
     const float2 aE0 = pr(8), aE1 = pr(9), aE2 = pr(10), aB0 = pr(11), aB1 = pr(12), aB2 = pr(13);
@@ -1074,7 +1077,8 @@ __global__ void __launch_bounds__(128)
     const float2 naB0 = make_float2(-aB0.x, -aB0.y), naB1 = make_float2(-aB1.x, -aB1.y),
                  naB2 = make_float2(-aB2.x, -aB2.y);
     const float2 igp = make_float2(1.f / gp.x, 1.f / gp.y);
-    double acc0[6] = {0, 0, 0, 0, 0, 0}, acc1[6] = {0, 0, 0, 0, 0, 0};  // gx(3), gu(3)
+#pragma unroll
+    for (int q = 0; q < 12; ++q) s_acc[q][tid] = 0.0;
     if (tid == 0) {
       wk = 0;
       woff = 0;
@@ -1093,7 +1097,9 @@ __global__ void __launch_bounds__(128)
       if (ok && act0) {
         const int cnt = s_cnt[bb], fl = s_flag[bb];
         const double scx = s_centre[bb][0], scy = s_centre[bb][1], scz = s_centre[bb][2];
-        const double dx0 = X0 - scx, dy0 = Y0 - scy, dz0 = Z0 - scz, dx1 = X1 - scx, dy1 = Y1 - scy, dz1 = Z1 - scz;
+        // the targets' FP64 coordinates (re-read per tile: L1-resident, saves registers)
+        const double dx0 = r0[0] - scx, dy0 = r0[1] - scy, dz0 = r0[2] - scz;
+        const double dx1 = r1[0] - scx, dy1 = r1[1] - scy, dz1 = r1[2] - scz;
         const float2 xh = make_float2((float)dx0, (float)dx1), yh = make_float2((float)dy0, (float)dy1),
                      zh = make_float2((float)dz0, (float)dz1);
         const float2 xl = make_float2((float)(dx0 - (double)xh.x), (float)(dx1 - (double)xh.y));
@@ -1163,19 +1169,23 @@ __global__ void __launch_bounds__(128)
         const float2 part[6] = {gx0, gx1, gx2, gu0, gu1, gu2};
 #pragma unroll
         for (int q = 0; q < 6; ++q) {
-          acc0[q] += (double)part[q].x;
-          acc1[q] += (double)part[q].y;
+          s_acc[q][tid] += (double)part[q].x;
+          s_acc[6 + q][tid] += (double)part[q].y;
         }
       }
       __syncthreads();  // buffer bb is refilled two iterations later
     }
+    double acc0[6], acc1[6];
 #pragma unroll
-    for (int q = 0; q < 6; ++q)
+    for (int q = 0; q < 6; ++q) {
+      acc0[q] = s_acc[q][tid];
+      acc1[q] = s_acc[6 + q][tid];
 #pragma unroll
       for (int o = 1; o < G; o <<= 1) {
         acc0[q] += __shfl_xor_sync(0xffffffffu, acc0[q], o);
         acc1[q] += __shfl_xor_sync(0xffffffffu, acc1[q], o);
       }
+    }
     if (g == 0) {
 #pragma unroll
       for (int q = 0; q < 6; ++q) {
@@ -1253,7 +1263,7 @@ int run_backward_t(Ctx *ctx, const double *d_ge, const double *d_gb, double *d_g
   double *adj, *rec16, *gxu, *gloc, *gmom, *gbox, *gpp, *gpbar;
   int *invp;
   FMM_TRY(ctx->ensure("bwd_adj", 6 * (int64_t)N, &adj));
-  FMM_TRY(ctx->ensure("bwd_rec16", 16 * (int64_t)N, &rec16));
+  FMM_TRY(ctx->ensure("bwd_rec16", kRecB * (int64_t)N, &rec16));
   FMM_TRY(ctx->ensure("bwd_gxu", 6 * (int64_t)N, &gxu));
   FMM_TRY(ctx->ensure("bwd_gloc", 6 * NN * nc, &gloc));
   FMM_TRY(ctx->ensure("bwd_gmom", 4 * NN * nc, &gmom));
@@ -1339,7 +1349,7 @@ int run_backward_t(Ctx *ctx, const double *d_ge, const double *d_gb, double *d_g
   // P2P^T (G lanes per target particle as in the forward)
   if (ctx->precision == FMMB200_PRECISION_MIXED) {
     float4 *recb;
-    FMM_TRY(ctx->ensure("bwd_p2p_rec", 8 * (int64_t)N, &recb));
+    FMM_TRY(ctx->ensure("bwd_p2p_rec", 9 * (int64_t)N, &recb));
     adj_p2p_rec_kernel<<<ceil_div(N, 256), 256, 0, st>>>(N, ctx->get<float4>("prec32x2"), adj, recb);
     FMM_TRY(ctx->check_launch("adj_p2p_rec_kernel"));
     const int *pp = ctx->get<int>("p2pu_ptr"), *ps = ctx->get<int>("p2pu_src");
