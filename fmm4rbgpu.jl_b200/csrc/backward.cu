@@ -619,7 +619,7 @@ struct MBShape2 {
   static constexpr int RECF = ((10 * NN + 3) / 4) * 4;
   static constexpr int RAWB = RECF * 4;              // bytes of the FP32 part of a staged record
   static constexpr int REC = RAWB + NS * 8;          // ... followed by the node coordinates
-  static constexpr int NACC = 13;                    // per target: axf(3) axw(3) ap(3) aG aM(3)
+  static constexpr int NACC = 14;                    // per target: axf(3) axw(3) ap(3) aG aM(3) sp
   static constexpr int SMEM = 2 * REC + 5 * NN * 16 + 2 * NACC * BT * 8;
 };
 
@@ -644,7 +644,7 @@ __global__ void adj_rec32_kernel(int64_t nc, const float *__restrict__ mom32, co
 // Per target cluster over its union list, two target nodes per thread in the two
 // lanes of packed FP32x2 instructions; the quantities are those of m2l_bwd_kernel:
 //   c = [f1] (Gamma_b gE_a + gB_a x M_b) - [f2] (Gamma_a gE_b + gB_b x M_a)
-//   gx_a += f c - 3 f5 (R.c)(R + (p.R) p)            (accumulated as axf - 3 axw)
+//   gx_a += f c - 3 f5 (R.c)(R + (p.R) p)            (accumulated as axf - 3 (axw + sp p))
 //   gp   += [f1] -3 f5 (p.R)(R.c1) R                  (accumulated as -3 ap)
 //   gGamma_a -= [f2] f gE_b.R,  gM_a -= [f2] f R x gB_b
 // Per source the FP32 partial sums are added into per-thread FP64 sums in shared memory.
@@ -747,7 +747,7 @@ __global__ void __launch_bounds__(MBShape2<NDEG>::BT)
         }
         const float2 z = make_float2(0.f, 0.f);
         float2 axf0 = z, axf1 = z, axf2 = z, axw0 = z, axw1 = z, axw2 = z, ap0 = z, ap1 = z, ap2 = z;
-        float2 aG = z, aM0 = z, aM1 = z, aM2 = z;
+        float2 aG = z, aM0 = z, aM1 = z, aM2 = z, sp = z;
         auto sweep = [&](auto FL) {
           constexpr int F = decltype(FL)::value;
 #pragma unroll 1
@@ -790,13 +790,10 @@ __global__ void __launch_bounds__(MBShape2<NDEG>::BT)
                 if constexpr ((F & 2) != 0) {
                   const float4 q2 = pb[5 * bi + 2], q3 = pb[5 * bi + 3], q4 = pb[5 * bi + 4];
                   const float2 E0 = lo2(q2), E1 = hi2(q2), E2 = lo2(q3), H0 = hi2(q3), H1 = lo2(q4), H2 = hi2(q4);
-                  const float2 d0 = fma2(nGa, E0, fma2(Ma1, H2, mul2(nMa2, H1)));
-                  const float2 d1 = fma2(nGa, E1, fma2(Ma2, H0, mul2(nMa0, H2)));
-                  const float2 d2 = fma2(nGa, E2, fma2(Ma0, H1, mul2(nMa1, H0)));
-                  c0 = add2(c0, d0);
-                  c1 = add2(c1, d1);
-                  c2 = add2(c2, d2);
-                  rc = fma2(rz, d2, fma2(ry, d1, fma2(rx, d0, rc)));
+                  c0 = fma2(nGa, E0, fma2(Ma1, H2, fma2(nMa2, H1, c0)));
+                  c1 = fma2(nGa, E1, fma2(Ma2, H0, fma2(nMa0, H2, c1)));
+                  c2 = fma2(nGa, E2, fma2(Ma0, H1, fma2(nMa1, H0, c2)));
+                  rc = fma2(rz, c2, fma2(ry, c1, mul2(rx, c0)));
                   const float2 er = fma2(rz, E2, fma2(ry, E1, mul2(rx, E0)));
                   aG = fma2(f, er, aG);
                   aM0 = fma2(f, fma2(ry, H2, mul2(nrz, H1)), aM0);
@@ -807,15 +804,16 @@ __global__ void __launch_bounds__(MBShape2<NDEG>::BT)
                 axf0 = fma2(f, c0, axf0);
                 axf1 = fma2(f, c1, axf1);
                 axf2 = fma2(f, c2, axf2);
-                axw0 = fma2(fr, fma2(tt, px, rx), axw0);
-                axw1 = fma2(fr, fma2(tt, py, ry), axw1);
-                axw2 = fma2(fr, fma2(tt, pz, rz), axw2);
+                axw0 = fma2(fr, rx, axw0);
+                axw1 = fma2(fr, ry, axw1);
+                axw2 = fma2(fr, rz, axw2);
+                sp = fma2(fr, tt, sp);  // the (p.R) p part: p is the same for every evaluation
               }
             }
           }
         };
         if (fl != 0) sweep(std::integral_constant<int, 3>{});
-        const float2 part[NACC] = {axf0, axf1, axf2, axw0, axw1, axw2, ap0, ap1, ap2, aG, aM0, aM1, aM2};
+        const float2 part[NACC] = {axf0, axf1, axf2, axw0, axw1, axw2, ap0, ap1, ap2, aG, aM0, aM1, aM2, sp};
 #pragma unroll
         for (int q = 0; q < NACC; ++q) {
           s_acc[(2 * q) * BT + tid] += (double)part[q].x;
@@ -844,7 +842,7 @@ __global__ void __launch_bounds__(MBShape2<NDEG>::BT)
       const int idx[3] = {a % M, (a / M) % M, a / (M * M)};
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
-        const double gx = v[d] - 3.0 * v[3 + d];
+        const double gx = v[d] - 3.0 * (v[3 + d] + v[13] * consts[d]);
         gbx[d] += (1.0 - ct.t[idx[d]]) * gx;
         gbx[3 + d] += ct.t[idx[d]] * gx;
         gpv[d] += -3.0 * v[6 + d];
@@ -1024,7 +1022,7 @@ __global__ void __launch_bounds__(128)
   __shared__ int s_cnt[2], s_flag[2];
   __shared__ double s_centre[2][3];
   __shared__ int s_warp[33];
-  __shared__ double s_acc[12][128];  // per thread: gx(3), gu(3) of both targets, FP64
+  __shared__ double s_acc[14][128];  // per thread: gx(3), gu(3), sw of both targets, FP64
   const int tid = threadIdx.x, TG = blockDim.x / G, tl = tid / G, g = tid % G;
   const int c = leaf0 + blockIdx.x;
   const int tlo = lohi[2 * c], thi = lohi[2 * c + 1], tcnt = thi - tlo + 1;
@@ -1078,7 +1076,7 @@ __global__ void __launch_bounds__(128)
                  naB2 = make_float2(-aB2.x, -aB2.y);
     const float2 igp = make_float2(1.f / gp.x, 1.f / gp.y);
 #pragma unroll
-    for (int q = 0; q < 12; ++q) s_acc[q][tid] = 0.0;
+    for (int q = 0; q < 14; ++q) s_acc[q][tid] = 0.0;
     if (tid == 0) {
       wk = 0;
       woff = 0;
@@ -1105,7 +1103,7 @@ __global__ void __launch_bounds__(128)
         const float2 xl = make_float2((float)(dx0 - (double)xh.x), (float)(dx1 - (double)xh.y));
         const float2 yl = make_float2((float)(dy0 - (double)yh.x), (float)(dy1 - (double)yh.y));
         const float2 zl = make_float2((float)(dz0 - (double)zh.x), (float)(dz1 - (double)zh.y));
-        float2 gx0 = z, gx1 = z, gx2 = z, gu0 = z, gu1 = z, gu2 = z;
+        float2 gx0 = z, gx1 = z, gx2 = z, gu0 = z, gu1 = z, gu2 = z, sw = z;
         const float4 *S = &buf[bb][0];
         auto sweep = [&](auto FL) {
           constexpr int F = decltype(FL)::value;
@@ -1149,10 +1147,11 @@ __global__ void __launch_bounds__(128)
               const float2 k2 = fma2(gp, e2, fma2(h0, up1, mul2(h1, nup0)));
               const float2 rk = fma2(rz, k2, fma2(ry, k1, mul2(rx, k0)));
               const float2 w = mul2(mul2(f, mul2(s2, rk)), three);  // 3 f5 (R.k)
-              gx0 = fma2(w, fma2(ur, up0, rx), fma2(nf, k0, gx0));
-              gx1 = fma2(w, fma2(ur, up1, ry), fma2(nf, k1, gx1));
-              gx2 = fma2(w, fma2(ur, up2, rz), fma2(nf, k2, gx2));
               const float2 wu = mul2(w, ur);
+              gx0 = fma2(w, rx, fma2(nf, k0, gx0));  // + w (R + (u_p.R) u_p): the u_p part as sum(wu) u_p
+              gx1 = fma2(w, ry, fma2(nf, k1, gx1));
+              gx2 = fma2(w, rz, fma2(nf, k2, gx2));
+              sw = add2(sw, wu);
               const float2 er = mul2(mul2(fma2(rz, e2, fma2(ry, e1, mul2(rx, e0))), nf), igp);
               gu0 = fma2(nf, sub2(mul2(ry, h2), mul2(rz, h1)), fma2(er, up0, fma2(wu, rx, gu0)));
               gu1 = fma2(nf, sub2(mul2(rz, h0), mul2(rx, h2)), fma2(er, up1, fma2(wu, ry, gu1)));
@@ -1166,20 +1165,21 @@ __global__ void __launch_bounds__(128)
           sweep(std::integral_constant<int, 1>{});
         else if (fl == 2)
           sweep(std::integral_constant<int, 2>{});
-        const float2 part[6] = {gx0, gx1, gx2, gu0, gu1, gu2};
+        const float2 part[7] = {gx0, gx1, gx2, gu0, gu1, gu2, sw};
 #pragma unroll
-        for (int q = 0; q < 6; ++q) {
+        for (int q = 0; q < 7; ++q) {
           s_acc[q][tid] += (double)part[q].x;
-          s_acc[6 + q][tid] += (double)part[q].y;
+          s_acc[7 + q][tid] += (double)part[q].y;
         }
       }
       __syncthreads();  // buffer bb is refilled two iterations later
     }
     double acc0[6], acc1[6];
+    const double sw0 = s_acc[6][tid], sw1 = s_acc[13][tid];
 #pragma unroll
     for (int q = 0; q < 6; ++q) {
-      acc0[q] = s_acc[q][tid];
-      acc1[q] = s_acc[6 + q][tid];
+      acc0[q] = s_acc[q][tid] + (q < 3 ? sw0 * r0[4 + q] : 0.0);
+      acc1[q] = s_acc[7 + q][tid] + (q < 3 ? sw1 * r1[4 + q] : 0.0);
 #pragma unroll
       for (int o = 1; o < G; o <<= 1) {
         acc0[q] += __shfl_xor_sync(0xffffffffu, acc0[q], o);
