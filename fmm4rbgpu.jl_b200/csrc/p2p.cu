@@ -24,6 +24,8 @@
 // records (80 bytes) hold every value duplicated, so that a 128-bit shared load
 // yields two packed operands.  Per-tile partial sums are folded into
 // Kahan-compensated FP32 accumulators; the output is FP64.
+#include <type_traits>
+
 #include "device_util.cuh"
 #include "kernels.cuh"
 #include "packed.cuh"
@@ -199,13 +201,14 @@ __global__ void __launch_bounds__(128) p2p_x2_kernel(const int *__restrict__ lea
   constexpr int REC = 5;  // float4 per source record
   __shared__ __align__(16) float4 buf[2][kP2PTile * REC];
   __shared__ __align__(8) uint64_t bar[2];
-  __shared__ int s_cnt[2];
+  __shared__ int s_cnt[2], s_near[2];
   __shared__ double s_centre[2][3];
   __shared__ int s_warp[33];
 
   const int tid = threadIdx.x, BT = blockDim.x, TG = BT / G;
   const int tl = tid / G, g = tid % G;
   const int c = leaf_ids ? leaf_ids[blockIdx.x] : leaf0 + blockIdx.x;
+  const double *tbox = bbox + 6 * (int64_t)c;
   const int tlo = lohi[2 * c], thi = lohi[2 * c + 1], tcnt = thi - tlo + 1;
   const int p0 = ptr[c], np = ptr[c + 1] - p0;
   const int W = count_tiles(lohi, src, p0, np, s_warp);
@@ -226,6 +229,14 @@ __global__ void __launch_bounds__(128) p2p_x2_kernel(const int *__restrict__ lea
     s_centre[bb][0] = 0.5 * (sb[0] + sb[3]);
     s_centre[bb][1] = 0.5 * (sb[1] + sb[4]);
     s_centre[bb][2] = 0.5 * (sb[2] + sb[5]);
+    // Boxes whose gap exceeds 1/8 of the larger extent: every pair difference is at least
+    // that gap, so the hi parts alone give R to ~9 FP32 ulps and the lo parts are skipped.
+    double gap = 0.0, ext = 0.0;
+    for (int d = 0; d < 3; ++d) {
+      gap = fmax(gap, fmax(sb[d] - tbox[3 + d], tbox[d] - sb[3 + d]));
+      ext = fmax(ext, fmax(sb[3 + d] - sb[d], tbox[3 + d] - tbox[d]));
+    }
+    s_near[bb] = !(8.0 * gap > ext);
     const uint32_t bytes = (uint32_t)(cnt * REC * sizeof(float4));
     mbar_arrive_expect_tx(&bar[bb], bytes);
     bulk_g2s(&buf[bb][0], rec_x2 + (int64_t)first * REC, bytes, &bar[bb]);
@@ -271,14 +282,24 @@ __global__ void __launch_bounds__(128) p2p_x2_kernel(const int *__restrict__ lea
         float2 e0 = make_float2(0.f, 0.f), e1 = e0, e2 = e0, bp0 = e0, bp1 = e0, bp2 = e0, bm0 = e0, bm1 = e0,
                bm2 = e0;
         const float4 *S = &buf[bb][0];
+        auto sweep = [&](auto NEARC) {
+          constexpr bool NEAR = decltype(NEARC)::value;
 #pragma unroll 2
         for (int j = g; j < cnt; j += G) {
           const float4 *r = S + j * REC;
-          const float4 r0 = r[0], r1 = r[1], r2 = r[2], r3 = r[3], r4 = r[4];
+          const float4 r0 = r[0], r1 = r[1], r3 = r[3], r4 = r[4];
           // R = (target hi - source hi) + (target lo - source lo); the record holds -hi, -lo
-          const float2 rx = add2(add2(xh, lo2(r0)), add2(xl, hi2(r1)));
-          const float2 ry = add2(add2(yh, hi2(r0)), add2(yl, lo2(r2)));
-          const float2 rz = add2(add2(zh, lo2(r1)), add2(zl, hi2(r2)));
+          float2 rx, ry, rz;
+          if constexpr (NEAR) {
+            const float4 r2 = r[2];
+            rx = add2(add2(xh, lo2(r0)), add2(xl, hi2(r1)));
+            ry = add2(add2(yh, hi2(r0)), add2(yl, lo2(r2)));
+            rz = add2(add2(zh, lo2(r1)), add2(zl, hi2(r2)));
+          } else {
+            rx = add2(xh, lo2(r0));
+            ry = add2(yh, hi2(r0));
+            rz = add2(zh, lo2(r1));
+          }
           const float2 gam = lo2(r3), ux = hi2(r3), uy = lo2(r4), uz = hi2(r4);
           const float2 rre = fma2(rx, rx, fma2(ry, ry, fma2(rz, rz, eps)));
           const float2 pr = fma2(uz, rz, fma2(uy, ry, mul2(ux, rx)));
@@ -297,6 +318,11 @@ __global__ void __launch_bounds__(128) p2p_x2_kernel(const int *__restrict__ lea
           bp2 = fma2(hx, ry, bp2);
           bm2 = fma2(hy, rx, bm2);
         }
+        };
+        if (s_near[bb])
+          sweep(std::integral_constant<bool, true>{});
+        else
+          sweep(std::integral_constant<bool, false>{});
         kahan_add2(ks[0], kc[0], e0);
         kahan_add2(ks[1], kc[1], e1);
         kahan_add2(ks[2], kc[2], e2);
