@@ -19,8 +19,8 @@
 // FP64 form (m2l_kernel): double throughout, one target node per thread.
 // Mixed form (m2l_x2_kernel): FP32 moments and arithmetic in packed FP32x2
 // instructions, two target nodes per thread in the two lanes of a float2; the
-// node offsets are formed in FP64 and rounded, and per-source partial sums are
-// folded into Kahan-compensated FP32 accumulators.
+// node offsets are formed in FP64 and rounded, and per-source FP32 partial sums
+// are added into per-thread FP64 sums held in shared memory.
 //
 // Mixed form on the tensor cores (m2l_tc_kernel, degree n <= 4, eta <= 1/2; an
 // opt-in engine -- at n = 4 it measures ~110 ms against ~99 ms for the packed
@@ -36,7 +36,7 @@
 // D += [K_hi; K_lo] x [V_hi | V_lo] (M = 128, N = 32, K = 8) against V held in
 // shared memory.  After each source D is read back (tcgen05.ld), its four
 // hi/lo products are summed and E = x'G - Q, B = W x x' - V is folded into
-// Kahan-compensated FP32 accumulators as in the CUDA-core form.
+// Kahan-compensated FP32 accumulators.
 #include "device_util.cuh"
 #include "kernels.cuh"
 #include "packed.cuh"
@@ -229,7 +229,8 @@ struct M2LShape2 {
   static constexpr int TPP = (NP + 511) / 512;        // pairs per thread
   static constexpr int BT = (((NP + TPP - 1) / TPP) + 31) / 32 * 32;
   static constexpr int REC = 4 * NN * 4 + NS * 8;     // raw FP32 moments then node coordinates
-  static constexpr int SMEM = 2 * REC + 5 * NN * 16;  // double buffer + packed node data (MASK uses 2/5)
+  // double buffer + packed node data (MASK uses 2/5) + per-thread FP64 sums of E, B of both targets
+  static constexpr int SMEM = 2 * REC + 5 * NN * 16 + TPP * 12 * BT * 8;
 };
 
 template <int NDEG, bool MASK>
@@ -242,6 +243,8 @@ __global__ void __launch_bounds__(M2LShape2<NDEG>::BT)
   constexpr int MOM_BYTES = 4 * NN * 4;
   extern __shared__ __align__(16) unsigned char smem[];
   float4 *pk = (float4 *)(smem + 2 * REC);  // 5*NN packed entries
+  // [q][c][BT]: c < 6 the first target's E, B, c >= 6 the second's (FP64 sums over sources)
+  double *s_acc = (double *)(smem + 2 * REC + 5 * NN * 16);
   __shared__ __align__(8) uint64_t bar[2];
   __shared__ double s_sn[3 * M];  // source node offsets from the target centre
 
@@ -252,12 +255,12 @@ __global__ void __launch_bounds__(M2LShape2<NDEG>::BT)
   const double *tb = bbox + 6 * (int64_t)t;
   const double cx = 0.5 * (tb[0] + tb[3]), cy = 0.5 * (tb[1] + tb[4]), cz = 0.5 * (tb[2] + tb[5]);
 
-  // per pair: E(3), B(3) of both targets as Kahan (sum, compensation) pairs
-  float2 ks[TPP][6], kc[TPP][6];
-#pragma unroll
-  for (int q = 0; q < TPP; ++q)
-#pragma unroll
-    for (int c = 0; c < 6; ++c) ks[q][c] = kc[q][c] = make_float2(0.f, 0.f);
+  for (int e = 0; e < TPP * 12; ++e) s_acc[e * BT + tid] = 0.0;
+  // one source's FP32 partial sums (both targets) into the FP64 sums
+  auto fold = [&](int q, int c, float2 v) {
+    s_acc[(q * 12 + c) * BT + tid] += (double)v.x;
+    s_acc[(q * 12 + 6 + c) * BT + tid] += (double)v.y;
+  };
 
   if (np > 0) {
     if (tid == 0) {
@@ -384,23 +387,23 @@ __global__ void __launch_bounds__(M2LShape2<NDEG>::BT)
             }
             if constexpr (MASK) {
               // coincident nodes are admissible: the factored form would cancel catastrophically
-              kahan_add2(ks[q][0], kc[q][0], g0);
-              kahan_add2(ks[q][1], kc[q][1], q0);
-              kahan_add2(ks[q][2], kc[q][2], q1);
-              kahan_add2(ks[q][3], kc[q][3], w0);
-              kahan_add2(ks[q][4], kc[q][4], w1);
-              kahan_add2(ks[q][5], kc[q][5], w2);
+              fold(q, 0, g0);
+              fold(q, 1, q0);
+              fold(q, 2, q1);
+              fold(q, 3, w0);
+              fold(q, 4, w1);
+              fold(q, 5, w2);
             } else {
               // this source's E and B at both nodes: E = x' G - Q, B = W x x' - V, folded per
               // source into the compensated sums
               const float2 xa = make_float2((float)tx0, (float)tx1), ya = make_float2((float)ty0, (float)ty1),
                            za = make_float2((float)tz0, (float)tz1);
-              kahan_add2(ks[q][0], kc[q][0], sub2(mul2(xa, g0), q0));
-              kahan_add2(ks[q][1], kc[q][1], sub2(mul2(ya, g0), q1));
-              kahan_add2(ks[q][2], kc[q][2], sub2(mul2(za, g0), q2));
-              kahan_add2(ks[q][3], kc[q][3], sub2(sub2(mul2(w1, za), mul2(w2, ya)), v0));
-              kahan_add2(ks[q][4], kc[q][4], sub2(sub2(mul2(w2, xa), mul2(w0, za)), v1));
-              kahan_add2(ks[q][5], kc[q][5], sub2(sub2(mul2(w0, ya), mul2(w1, xa)), v2));
+              fold(q, 0, sub2(mul2(xa, g0), q0));
+              fold(q, 1, sub2(mul2(ya, g0), q1));
+              fold(q, 2, sub2(mul2(za, g0), q2));
+              fold(q, 3, sub2(sub2(mul2(w1, za), mul2(w2, ya)), v0));
+              fold(q, 4, sub2(sub2(mul2(w2, xa), mul2(w0, za)), v1));
+              fold(q, 5, sub2(sub2(mul2(w0, ya), mul2(w1, xa)), v2));
             }
           }
         }
@@ -415,11 +418,11 @@ __global__ void __launch_bounds__(M2LShape2<NDEG>::BT)
     if (k < NP) {
 #pragma unroll
       for (int c = 0; c < 6; ++c) {
-        float o0 = (float)((double)ks[q][c].x - (double)kc[q][c].x);
+        float o0 = (float)s_acc[(q * 12 + c) * BT + tid];
         if (accumulate) o0 += out[c * NN + k];
         out[c * NN + k] = o0;
         if (k + NP < NN) {
-          float o1 = (float)((double)ks[q][c].y - (double)kc[q][c].y);
+          float o1 = (float)s_acc[(q * 12 + 6 + c) * BT + tid];
           if (accumulate) o1 += out[c * NN + k + NP];
           out[c * NN + k + NP] = o1;
         }
