@@ -22,8 +22,8 @@
 // ~1 ulp of |R| even for very close pairs (the hi difference is exact,
 // Sterbenz), which a plain FP32 leaf-local coordinate cannot give.  Source
 // records (80 bytes) hold every value duplicated, so that a 128-bit shared load
-// yields two packed operands.  Per-tile partial sums are folded into
-// Kahan-compensated FP32 accumulators; the output is FP64.
+// yields two packed operands.  Per-tile FP32 partial sums are added into per-thread
+// FP64 sums in shared memory; the output is FP64.
 #include <type_traits>
 
 #include "device_util.cuh"
@@ -204,6 +204,7 @@ __global__ void __launch_bounds__(128) p2p_x2_kernel(const int *__restrict__ lea
   __shared__ int s_cnt[2], s_near[2];
   __shared__ double s_centre[2][3];
   __shared__ int s_warp[33];
+  __shared__ double s_acc[12][128];  // per thread: E, B of both targets, FP64 sums over tiles
 
   const int tid = threadIdx.x, BT = blockDim.x, TG = BT / G;
   const int tl = tid / G, g = tid % G;
@@ -250,9 +251,8 @@ __global__ void __launch_bounds__(128) p2p_x2_kernel(const int *__restrict__ lea
     // FP64 target coordinates of both targets
     const double X0 = prec64[pj0 * 8 + 0], Y0 = prec64[pj0 * 8 + 1], Z0 = prec64[pj0 * 8 + 2];
     const double X1 = prec64[pj1 * 8 + 0], Y1 = prec64[pj1 * 8 + 1], Z1 = prec64[pj1 * 8 + 2];
-    float2 ks[6], kc[6];
 #pragma unroll
-    for (int q = 0; q < 6; ++q) ks[q] = kc[q] = make_float2(0.f, 0.f);
+    for (int q = 0; q < 12; ++q) s_acc[q][tid] = 0.0;
     if (tid == 0) {
       cur = TileCursor{0, 0};
       if (W > 0) {
@@ -323,12 +323,12 @@ __global__ void __launch_bounds__(128) p2p_x2_kernel(const int *__restrict__ lea
           sweep(std::integral_constant<bool, true>{});
         else
           sweep(std::integral_constant<bool, false>{});
-        kahan_add2(ks[0], kc[0], e0);
-        kahan_add2(ks[1], kc[1], e1);
-        kahan_add2(ks[2], kc[2], e2);
-        kahan_add2(ks[3], kc[3], sub2(bp0, bm0));
-        kahan_add2(ks[4], kc[4], sub2(bp1, bm1));
-        kahan_add2(ks[5], kc[5], sub2(bp2, bm2));
+        const float2 part[6] = {e0, e1, e2, sub2(bp0, bm0), sub2(bp1, bm1), sub2(bp2, bm2)};
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+          s_acc[q][tid] += (double)part[q].x;
+          s_acc[6 + q][tid] += (double)part[q].y;
+        }
       }
       __syncthreads();  // buffer bb is refilled two iterations later
     }
@@ -336,8 +336,8 @@ __global__ void __launch_bounds__(128) p2p_x2_kernel(const int *__restrict__ lea
     double v0[6], v1[6];
 #pragma unroll
     for (int q = 0; q < 6; ++q) {
-      v0[q] = (double)ks[q].x - (double)kc[q].x;
-      v1[q] = (double)ks[q].y - (double)kc[q].y;
+      v0[q] = s_acc[q][tid];
+      v1[q] = s_acc[6 + q][tid];
 #pragma unroll
       for (int o = 1; o < G; o <<= 1) {
         v0[q] += __shfl_xor_sync(0xffffffffu, v0[q], o);
