@@ -263,6 +263,9 @@ __global__ void __launch_bounds__(Grid<NDEG>::BT)
 
 // ---------------------------------------------------------------- L2P
 // mode 0: near[q][p] += far (tree order); mode 1: out[perm[p]] = amp*(near + far).
+// Two threads per particle: h = 0 evaluates the E components, h = 1 the B
+// components of the leaf's local expansion, as three independent accumulation
+// chains over the tensor-product grid.
 template <int NDEG, bool MIXED>
 __global__ void __launch_bounds__(128)
     l2p_kernel(const int *__restrict__ leaf_ids, int leaf0, const int *__restrict__ lohi,
@@ -277,6 +280,7 @@ __global__ void __launch_bounds__(128)
   __shared__ double s_n64[3 * M];
   __shared__ float s_n32[3 * M];
   const int tid = threadIdx.x;
+  const int h = tid & 1;
   const int c = leaf_ids ? leaf_ids[blockIdx.x] : leaf0 + blockIdx.x;
   const int lo = lohi[2 * c], hi = lohi[2 * c + 1];
   const double *bb = bbox + 6 * (int64_t)c;
@@ -289,48 +293,51 @@ __global__ void __launch_bounds__(128)
     s_n32[i] = (float)(v - 0.5 * (bb[d] + bb[3 + d]));
   }
   __syncthreads();
-  for (int p = lo + tid; p <= hi; p += blockDim.x) {
+  const T *L0 = s_loc + (3 * h) * NN, *L1 = L0 + NN, *L2 = L1 + NN;
+  for (int p = lo + (tid >> 1); p <= hi; p += blockDim.x >> 1) {
     T wx[M], wy[M], wz[M];
     if constexpr (MIXED) {
       const float *r = (const float *)prec_v + (int64_t)p * 8;
-      weights32<M>(r[0], s_n32, wx);
-      weights32<M>(r[1], s_n32 + M, wy);
-      weights32<M>(r[2], s_n32 + 2 * M, wz);
+      weights32_fast<M>(r[0], s_n32, wx);
+      weights32_fast<M>(r[1], s_n32 + M, wy);
+      weights32_fast<M>(r[2], s_n32 + 2 * M, wz);
     } else {
       const double *r = (const double *)prec_v + (int64_t)p * 8;
       weights64<M>(r[0], s_n64, wx);
       weights64<M>(r[1], s_n64 + M, wy);
       weights64<M>(r[2], s_n64 + 2 * M, wz);
     }
-    double f[6];
+    T f0 = 0, f1 = 0, f2 = 0;
+#pragma unroll 1
+    for (int k = 0; k < M; ++k) {
+      T y0 = 0, y1 = 0, y2 = 0;
 #pragma unroll
-    for (int q = 0; q < 6; ++q) {
-      const T *L = s_loc + q * NN;
-      T vz = 0;
-      for (int k = 0; k < M; ++k) {
-        T vy = 0;
+      for (int j = 0; j < M; ++j) {
+        const int o = M * (j + M * k);
+        T x0 = 0, x1 = 0, x2 = 0;
 #pragma unroll
-        for (int j = 0; j < M; ++j) {
-          const T *row = L + M * (j + M * k);
-          T vx = 0;
-#pragma unroll
-          for (int i = 0; i < M; ++i) vx += wx[i] * row[i];
-          vy += wy[j] * vx;
+        for (int i = 0; i < M; ++i) {
+          x0 += wx[i] * L0[o + i];
+          x1 += wx[i] * L1[o + i];
+          x2 += wx[i] * L2[o + i];
         }
-        vz += wz[k] * vy;
+        y0 += wy[j] * x0;
+        y1 += wy[j] * x1;
+        y2 += wy[j] * x2;
       }
-      f[q] = (double)vz;
+      f0 += wz[k] * y0;
+      f1 += wz[k] * y1;
+      f2 += wz[k] * y2;
     }
+    const double f[3] = {(double)f0, (double)f1, (double)f2};
     if (mode == 0) {
 #pragma unroll
-      for (int q = 0; q < 6; ++q) near[(int64_t)q * N + p] += f[q];
+      for (int q = 0; q < 3; ++q) near[(int64_t)(3 * h + q) * N + p] += f[q];
     } else {
       const int64_t o = 3 * (int64_t)perm[p];
+      double *out = h == 0 ? out_e : out_b;
 #pragma unroll
-      for (int q = 0; q < 3; ++q) {
-        out_e[o + q] = amp * (near[(int64_t)q * N + p] + f[q]);
-        out_b[o + q] = amp * (near[(int64_t)(q + 3) * N + p] + f[q + 3]);
-      }
+      for (int q = 0; q < 3; ++q) out[o + q] = amp * (near[(int64_t)(3 * h + q) * N + p] + f[q]);
     }
   }
 }

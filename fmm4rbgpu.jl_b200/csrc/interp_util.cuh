@@ -61,6 +61,31 @@ __device__ __forceinline__ void weights32(float x, const float *nodes, float *w)
   }
 }
 
+// As weights32 with the approximate FP32 division (__fdividef, ~2 ulp): the
+// normalisation by the sum of the q_i carries that error into every weight
+// alike, so the weights still sum to 1 to FP32 rounding.
+template <int M>
+__device__ __forceinline__ void weights32_fast(float x, const float *nodes, float *w) {
+  float q[M];
+  float sum = 0.f;
+  int flag = -1;
+#pragma unroll
+  for (int i = 0; i < M; ++i) {
+    const float dx = x - nodes[i];
+    flag = fabsf(dx) < 1.17549435e-38f ? i : flag;
+    q[i] = __fdividef((float)bary_ws(i, M), dx);
+    sum += q[i];
+  }
+  if (flag >= 0) {
+#pragma unroll
+    for (int i = 0; i < M; ++i) w[i] = i == flag ? 1.f : 0.f;
+  } else {
+    const float inv = __fdividef(1.f, sum);
+#pragma unroll
+    for (int i = 0; i < M; ++i) w[i] = q[i] * inv;
+  }
+}
+
 // Weights and their x-derivatives (FP64).  Off the nodes
 //   w_i' = w_i (S2/S - 1/(x - x_i)),  S = sum_j ws_j/(x-x_j), S2 = sum_j ws_j/(x-x_j)^2;
 // on node k the barycentric differentiation matrix row
