@@ -58,6 +58,9 @@ def parse():
     ap.add_argument("--N0", type=int, default=125)
     ap.add_argument("--eta", type=float, default=0.5)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--dist", choices=["gauss", "beamlets", "uniform"], default="gauss",
+                    help="gauss: the Gaussian bunch; beamlets: 8 Gaussian beamlets with centres U[-5,5]^3 "
+                         "(sigma=(0.3,0.3,0.03), u_z~N(100,0.1)); uniform: U[0,1]^3 at rest")
     ap.add_argument("--ntargets", type=int, default=4096)
     ap.add_argument("--cpu-sample", type=int, default=2**17, help="particles in the CPU-baseline sample")
     ap.add_argument("--ref-sample", type=int, default=2**18, help="particles per reference-arm step")
@@ -70,11 +73,25 @@ def parse():
     return ap.parse_args()
 
 
+DISTS = {
+    "gauss": "Gaussian bunch (sigma=(1,1,0.1), u_z~N(200,0.2), u_x,u_y~N(0,0.01))",
+    "beamlets": "8 Gaussian beamlets, centres U[-5,5]^3 (sigma=(0.3,0.3,0.03), u_z~N(100,0.1), u_x,u_y~N(0,0.005))",
+    "uniform": "uniform U[0,1]^3 at rest",
+}
+
+
+def generate(args, N, seed):
+    from fmmb200 import beams
+
+    gen = {"gauss": beams.gaussian_bunch, "beamlets": beams.beamlets, "uniform": beams.uniform}[args.dist]
+    return gen(N, seed=seed)
+
+
 def workload(args):
     return {
-        "workload": f"Gaussian bunch N={args.N} (sigma=(1,1,0.1), u_z~N(200,0.2), u_x,u_y~N(0,0.01)), "
+        "workload": f"{DISTS[args.dist]} N={args.N}, "
                     f"n={args.n}, N0={args.N0}, eta={args.eta}, lambda=1; value = mixed form, fp64 = plain path",
-        "npar": args.N, "n": args.n, "N0": args.N0, "eta": args.eta, "lambda": 1.0,
+        "npar": args.N, "n": args.n, "N0": args.N0, "eta": args.eta, "lambda": 1.0, "dist": args.dist,
         "l2": "inputs larger than L2 (AoS positions+momenta 48 B/particle resident in HBM; no flush)",
     }
 
@@ -179,7 +196,7 @@ def run_reference(args, world, rank):
 
     nthreads = os.cpu_count() or 1
     N = min(args.ref_sample, args.N)
-    pos, mom = beams.gaussian_bunch(N, seed=args.seed)
+    pos, mom = generate(args, N, args.seed)
     for _ in range(args.warmup):
         oracle.fmm(pos, mom, -1.0, 1.0, args.n, args.N0, args.eta, nthreads=nthreads)
     times = []
@@ -206,7 +223,7 @@ def cpu_baseline(args):
     from fmmb200 import beams
 
     N = min(args.cpu_sample, args.N)
-    pos, mom = beams.gaussian_bunch(N, seed=args.seed + 1)
+    pos, mom = generate(args, N, args.seed + 1)
     t0 = time.perf_counter()
     oracle.fmm(pos, mom, -1.0, 1.0, args.n, args.N0, args.eta, nthreads=1)
     t = time.perf_counter() - t0
@@ -224,7 +241,7 @@ def run_ours(args, world, rank, local):
 
     dev = torch.device("cuda", local)
     N = args.N
-    pos_h, mom_h = beams.gaussian_bunch(N, seed=args.seed + rank)
+    pos_h, mom_h = generate(args, N, args.seed + rank)
     pos = torch.from_numpy(pos_h).to(dev)
     mom = torch.from_numpy(mom_h).to(dev)
     E = torch.empty_like(pos)
@@ -298,6 +315,7 @@ def run_ours(args, world, rank, local):
 
     # forward + adjoint (the gradient path of the fields), device-resident
     fwd_bwd = None
+    bwd_bytes = None
     if not args.skip_backward:
         gen = torch.Generator(device=dev).manual_seed(args.seed + 7)
         gE = torch.randn((N, 3), dtype=torch.float64, device=dev, generator=gen)
@@ -324,6 +342,7 @@ def run_ours(args, world, rank, local):
             ev1.record(stream)
             ev1.synchronize()
             ms_fb = max_over_ranks(world, ev0.elapsed_time(ev1) / args.bwd_steps)
+            bwd_bytes = max(bwd_bytes or 0, int(ctx.stats()["device_bytes"]))
             fwd_bwd[name] = {"ms_per_step": ms_fb, "value": replicas.aggregate_rate(world, N, ms_fb),
                              "unit": "particles/s", "ratio_to_forward": ms_fb / ms_f, "steps": args.bwd_steps,
                              "warmup": 2, "grad_finite": bool(torch.isfinite(gx).all() and torch.isfinite(gu).all())}
@@ -403,7 +422,9 @@ def run_ours(args, world, rank, local):
                      "p2p_kernel_evals": st["p2p_kernel_evals"], "max_level": st["max_level"],
                      "ncluster": st["ncluster"], "model_flops_per_step": mf,
                      "model_tflops_mixed": mf / (ms_mixed * 1e-3) / 1e12,
-                     "model_tflops_fp64": mf / (ms_fp64 * 1e-3) / 1e12, "device_bytes": st["device_bytes"]},
+                     "model_tflops_fp64": mf / (ms_fp64 * 1e-3) / 1e12, "device_bytes": st["device_bytes"],
+                     "device_bytes_with_backward": bwd_bytes,
+                     "torch_peak_bytes": int(torch.cuda.max_memory_allocated(dev))},
             "fwd_bwd": fwd_bwd,
             "roofline": roof,
             "cpu_baseline": cpu,
