@@ -1007,9 +1007,11 @@ __global__ void adj_p2p_rec_kernel(int N, const float4 *__restrict__ prec32x2, c
 // Per target leaf over its union list, G lanes per pair of target particles, the
 // two targets in the two lanes of packed FP32x2 instructions (quantities as in
 // p2p_bwd_kernel).  R = x_p - x_j is formed in the source leaf's frame from hi + lo
-// parts as in the mixed forward; R = 0 (the particle itself, or a duplicate
-// position) contributes nothing, as in the forward.  Per tile the FP32 partial sums
-// are added into FP64 registers.
+// parts as in the mixed forward.  The particle itself is skipped, as in the FP64
+// adjoint; a distinct particle at the same position keeps the regularised
+// kernel's finite derivative (f = eps^-3/2 times c; the f5 term is formed as
+// f (s^2 (R.c)) and vanishes without overflowing).  Per tile the FP32 partial sums
+// are added into FP64 sums in shared memory.
 template <int G>
 __global__ void __launch_bounds__(128)
     p2p_bwd_x2_kernel(int leaf0, const int *__restrict__ lohi, const int *__restrict__ ptr,
@@ -1019,7 +1021,7 @@ __global__ void __launch_bounds__(128)
   constexpr int REC = 9;  // float4 per source record (the last one padding)
   __shared__ __align__(16) float4 buf[2][kPbTile * REC];
   __shared__ __align__(8) uint64_t bar[2];
-  __shared__ int s_cnt[2], s_flag[2];
+  __shared__ int s_cnt[2], s_flag[2], s_first[2];
   __shared__ double s_centre[2][3];
   __shared__ int s_warp[33];
   __shared__ double s_acc[14][128];  // per thread: gx(3), gu(3), sw of both targets, FP64
@@ -1047,6 +1049,7 @@ __global__ void __launch_bounds__(128)
     const int cnt = scnt - woff < kPbTile ? scnt - woff : kPbTile;
     s_cnt[bb] = cnt;
     s_flag[bb] = flg[p0 + wk];
+    s_first[bb] = slo + woff;
     const double *sb = bbox + 6 * (int64_t)s;
     s_centre[bb][0] = 0.5 * (sb[0] + sb[3]);
     s_centre[bb][1] = 0.5 * (sb[1] + sb[4]);
@@ -1094,6 +1097,7 @@ __global__ void __launch_bounds__(128)
       const bool ok = mbar_wait_bounded(&bar[bb], (uint32_t)((it >> 1) & 1), status);
       if (ok && act0) {
         const int cnt = s_cnt[bb], fl = s_flag[bb];
+        const int self0 = (int)pj0 - s_first[bb], self1 = (int)pj1 - s_first[bb];  // j of the targets themselves
         const double scx = s_centre[bb][0], scy = s_centre[bb][1], scz = s_centre[bb][2];
         // the targets' FP64 coordinates (re-read per tile: L1-resident, saves registers)
         const double dx0 = r0[0] - scx, dy0 = r0[1] - scy, dz0 = r0[2] - scz;
@@ -1121,8 +1125,8 @@ __global__ void __launch_bounds__(128)
               const float2 ur = fma2(uj2, rz, fma2(uj1, ry, mul2(uj0, rx)));
               const float2 d = fma2(ur, ur, add2(rr, eps));
               float2 sv = rsqrt2(d);
-              sv.x = rr.x > 0.f ? sv.x : 0.f;
-              sv.y = rr.y > 0.f ? sv.y : 0.f;
+              sv.x = j != self0 ? sv.x : 0.f;
+              sv.y = j != self1 ? sv.y : 0.f;
               const float2 s2 = mul2(sv, sv), f = mul2(s2, sv);
               const float2 k0 = fma2(gj, aE0, fma2(aB1, uj2, mul2(naB2, uj1)));
               const float2 k1 = fma2(gj, aE1, fma2(aB2, uj0, mul2(naB0, uj2)));
@@ -1139,8 +1143,8 @@ __global__ void __launch_bounds__(128)
               const float2 ur = fma2(up2, rz, fma2(up1, ry, mul2(up0, rx)));
               const float2 d = fma2(ur, ur, add2(rr, eps));
               float2 sv = rsqrt2(d);
-              sv.x = rr.x > 0.f ? sv.x : 0.f;
-              sv.y = rr.y > 0.f ? sv.y : 0.f;
+              sv.x = j != self0 ? sv.x : 0.f;
+              sv.y = j != self1 ? sv.y : 0.f;
               const float2 s2 = mul2(sv, sv), f = mul2(s2, sv), nf = make_float2(-f.x, -f.y);
               const float2 k0 = fma2(gp, e0, fma2(h1, up2, mul2(h2, nup1)));
               const float2 k1 = fma2(gp, e1, fma2(h2, up0, mul2(h0, nup2)));

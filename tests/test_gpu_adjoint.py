@@ -119,7 +119,7 @@ def test_mixed_forward_adjoint_matches_fp64(gpu_ctx):
 
 @pytest.mark.parametrize("kind,N,n,N0,eta", [("gauss", 30000, 4, 125, 0.5), ("gauss", 30000, 4, 32, 0.5),
                                               ("uniform", 20000, 3, 100, 0.5), ("beamlets", 20000, 2, 200, 0.5),
-                                              ("gauss", 20000, 4, 64, 0.7)])
+                                              ("gauss", 20000, 4, 64, 0.7), ("duplicates", 20000, 4, 64, 0.5)])
 def test_mixed_adjoint_kernels_match_fp64(gpu_ctx, kind, N, n, N0, eta):
     """The mixed form's adjoint runs M2L^T and P2P^T in packed FP32 (hi/lo
     coordinates in the near field); it stays within 1e-4 of the FP64 adjoint for
@@ -127,8 +127,11 @@ def test_mixed_adjoint_kernels_match_fp64(gpu_ctx, kind, N, n, N0, eta):
     import fmmb200
     from fmmb200 import beams
 
-    gen = {"gauss": beams.gaussian_bunch, "uniform": beams.uniform, "beamlets": beams.beamlets}[kind]
+    gen = {"gauss": beams.gaussian_bunch, "uniform": beams.uniform, "beamlets": beams.beamlets,
+           "duplicates": beams.gaussian_bunch}[kind]
     pos, mom = gen(N, seed=4)
+    if kind == "duplicates":  # twins at one position: the regularised kernel's derivative at R = 0
+        pos[1::2] = pos[0::2]
     if kind == "uniform":
         mom = np.random.default_rng(5).normal(0, 0.5, (N, 3))  # nonzero momenta: B and d/du are exercised
     rng = np.random.default_rng(2)

@@ -46,6 +46,83 @@ def test_fp64_matches_oracle_fmm(gpu_ctx, oracle_mod, N, kind, n, N0):
     assert (i["nm2l"], i["np2p"]) == (st["nm2l"], st["np2p"])
 
 
+def _degenerate(case, N, seed=0):
+    from fmmb200 import beams
+
+    pos, mom = beams.gaussian_bunch(N, seed=seed)
+    if case == "planar":  # every box has zero extent along z
+        pos[:, 2] = 0.0
+    elif case == "line":  # zero extent along y and z
+        pos[:, 1:] = 0.0
+    elif case == "duplicates":  # every particle has a twin at the same position
+        pos[1::2] = pos[0::2]
+    elif case == "identical":  # all at one point: nothing is admissible, every field is zero
+        pos[:] = 0.25
+    return pos, mom
+
+
+@pytest.mark.parametrize("case,N,n,N0", [("planar", 20000, 4, 64), ("line", 8000, 3, 50),
+                                         ("duplicates", 20000, 4, 64), ("identical", 1500, 2, 100)])
+def test_degenerate_inputs(gpu_ctx, oracle_mod, case, N, n, N0):
+    """Degenerate geometry (zero box extents, exact-node interpolation everywhere) and
+    coincident particles (R = 0 between distinct particles gives K = 0, as in the
+    reference's regularised kernel): FP64 against the oracle's FMMGPU variant, whose
+    exact-node rule the device follows (the serial reference's weights sum to n+1 on
+    coincident nodes, see test_coincident_nodes_weights), and mixed against FP64."""
+    import fmmb200
+
+    pos, mom = _degenerate(case, N)
+    alg = fmmb200.FMMB200(n=n, N0=N0, eta=0.5)
+    E, B = gpu_ctx.forward(pos, mom, alg)
+    Eo, Bo, st = oracle_mod.fmm(pos, mom, -1.0, 1.0, n, N0, 0.5, variant=oracle_mod.VARIANT_GPU,
+                                nthreads=NTHREADS)
+    i = gpu_ctx.tree_info()
+    assert (i["nm2l"], i["np2p"]) == (st["nm2l"], st["np2p"])
+    Em, Bm = gpu_ctx.forward(pos, mom, fmmb200.FMMB200(n=n, N0=N0, eta=0.5, precision="mixed"))
+    assert np.all(np.isfinite(Em)) and np.all(np.isfinite(Bm))
+    if case == "identical":
+        assert np.all(E == 0.0) and np.all(B == 0.0) and np.all(Eo == 0.0) and np.all(Em == 0.0)
+        return
+    assert rel(E, Eo) < FP64_TOL and rel(B, Bo) < FP64_TOL
+    assert rel(Em, E) < MIXED_TOL and rel(Bm, B) < MIXED_TOL
+    if case in ("planar", "line"):
+        Eb, _ = oracle_mod.bruteforce(pos, mom, -1.0, 1.0, NTHREADS)
+        # the FMM's truncation error on this flat beam (2.8e-2 planar at n = 4); the serial
+        # reference's all-ones weights on coincident nodes would be off by orders of magnitude
+        assert rel(E, Eb) < 0.1
+
+
+@pytest.mark.parametrize("N,kind,n,N0", [(20000, "gauss", 1, 40), (12000, "beamlets", 10, 200)])
+def test_extreme_degrees(gpu_ctx, oracle_mod, N, kind, n, N0):
+    import fmmb200
+
+    pos, mom = make(kind, N, 1)
+    E, B = gpu_ctx.forward(pos, mom, fmmb200.FMMB200(n=n, N0=N0, eta=0.5))
+    Eo, Bo, _ = oracle_mod.fmm(pos, mom, -1.0, 1.0, n, N0, 0.5, nthreads=NTHREADS)
+    assert rel(E, Eo) < FP64_TOL and rel(B, Bo) < FP64_TOL
+    Em, Bm = gpu_ctx.forward(pos, mom, fmmb200.FMMB200(n=n, N0=N0, eta=0.5, precision="mixed"))
+    # the 1e-5 target is stated for n = 4; with linear interpolation (n = 1) the mixed form's
+    # FP32 rounding measures 1.0e-5 on this case
+    tol = MIXED_TOL if n > 1 else 2e-5
+    assert rel(Em, E) < tol and rel(Bm, B) < tol
+
+
+@pytest.mark.parametrize("eta", [0.3, 0.7])
+def test_other_admissibility(gpu_ctx, oracle_mod, eta):
+    """eta = 0.7 admits coincident target/source nodes (masked kernel, non-factored mixed
+    M2L); eta = 0.3 shifts work from M2L to P2P."""
+    import fmmb200
+
+    pos, mom = make("gauss", 30000, 3)
+    E, B = gpu_ctx.forward(pos, mom, fmmb200.FMMB200(n=4, N0=64, eta=eta))
+    Eo, Bo, st = oracle_mod.fmm(pos, mom, -1.0, 1.0, 4, 64, eta, nthreads=NTHREADS)
+    assert rel(E, Eo) < FP64_TOL and rel(B, Bo) < FP64_TOL
+    i = gpu_ctx.tree_info()
+    assert (i["nm2l"], i["np2p"]) == (st["nm2l"], st["np2p"])
+    Em, Bm = gpu_ctx.forward(pos, mom, fmmb200.FMMB200(n=4, N0=64, eta=eta, precision="mixed"))
+    assert rel(Em, E) < MIXED_TOL and rel(Bm, B) < MIXED_TOL
+
+
 def test_config1_against_bruteforce(gpu_ctx, oracle_mod):
     """N=65,536 uniform, u=0, n=4, N0=125, eta=0.5: FMM truncation error vs BruteForce."""
     import fmmb200

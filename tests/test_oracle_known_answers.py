@@ -216,3 +216,33 @@ def test_empty_lists_give_empty_csr(oracle_mod):
     assert oracle_mod.ilistptrs(np.zeros((0, 2), np.int64)).tolist() == [0]
     ptrs = oracle_mod.ilistptrs(oracle_mod.sort_by_target([[2, 0], [0, 1], [2, 3], [0, 0]]))
     assert ptrs.tolist() == [0, 2, 4]
+
+
+def test_coincident_nodes_weights(oracle_mod):
+    """A box of zero extent makes all n+1 interpolation nodes coincide.  The serial
+    reference's lgweight (src/fmm/upwardpass.jl:6-9) then returns a weight of 1 on every
+    node (convert.(Float64, bitarr)), so its weights sum to n+1; the GPU kernels'
+    exact-node rule puts the single weight on the last matching node
+    (src/gpu_fmm/gpu_upwardpass.jl:52-54).  The oracle keeps both; the device follows
+    the second, which is the one that reproduces the direct sum on planar inputs."""
+    import numpy as np
+
+    nodes = np.full(5, 0.25)
+    w_cpu = oracle_mod.lgweight(0.25, nodes, gpu=False)
+    w_gpu = oracle_mod.lgweight(0.25, nodes, gpu=True)
+    assert np.array_equal(w_cpu, np.ones(5))
+    assert np.array_equal(w_gpu, np.array([0.0, 0.0, 0.0, 0.0, 1.0]))
+
+
+def test_planar_input_gpu_variant_matches_bruteforce(oracle_mod):
+    import numpy as np
+    from fmmb200 import beams
+
+    pos, mom = beams.gaussian_bunch(4000, seed=0)
+    pos[:, 2] = 0.0
+    Eb, _ = oracle_mod.bruteforce(pos, mom, -1.0, 1.0, 4)
+    Eg, _, _ = oracle_mod.fmm(pos, mom, -1.0, 1.0, 4, 64, 0.5, variant=oracle_mod.VARIANT_GPU, nthreads=4)
+    Ec, _, _ = oracle_mod.fmm(pos, mom, -1.0, 1.0, 4, 64, 0.5, variant=oracle_mod.VARIANT_CPU, nthreads=4)
+    err = lambda a: float(np.linalg.norm(a - Eb) / np.linalg.norm(Eb))  # noqa: E731
+    assert err(Eg) < 1e-3  # the FMM truncation error
+    assert err(Ec) > 1.0  # the serial reference's all-ones weights on coincident nodes
