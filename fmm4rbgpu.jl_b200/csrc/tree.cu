@@ -2,7 +2,9 @@
 // fillclusters!, src/cluster_tree/clusters.jl:21-70, on the host there).
 //
 // Design (B200): the three coordinate orders are radix-sorted once (64-bit
-// order-preserving keys, ties by particle id).  Level by level, every node's
+// order-preserving keys, ties by particle id).  Level by level (globally down to
+// the first level whose nodes hold at most 4096 particles, then per subtree in
+// shared memory, see subtree_kernel), every node's
 // bounding box is read off the ends of its three sorted segments (exact
 // min/max), the split axis is argmax(stretch .* extent) and the left child
 // takes the first ceil(cnt/2) particles of the split-axis segment -- the
@@ -317,6 +319,180 @@ __global__ void gather64_kernel(int N, const uint32_t *__restrict__ perm, const 
   r[3] = make_double2(uz, 0.0);
 }
 
+// ---------------------------------------------------------------- bottom levels in shared memory
+// One CTA per node of level L0 (at most kStCap particles) completes its subtree:
+// the node's three sorted lists are loaded once and renamed to local 16-bit ids
+// (one scatter and one gather through `lid`), then every remaining level reads
+// its boxes off the segment ends, flags the split-axis halves and partitions the
+// three lists stably with block scans -- the same steps, in the same order, as
+// the global levels.  At the leaves the particle ids are written in ascending
+// order (rank within the leaf), which replaces the final sort by leaf.
+constexpr int kStCap = 4096;
+constexpr int kStThreads = 256;
+constexpr int kStItems = kStCap / kStThreads;
+constexpr int kStMaxSub = 512;    // sub-nodes of one level that split (depth <= 9)
+constexpr int kStSmem = 2 * 3 * kStCap * 2 + kStCap * 4 + kStCap * 4 + kStCap;
+
+// Range of sub-node s (left to right) `depth` levels below [lo0, hi0].
+__device__ __forceinline__ void sub_range(int lo0, int hi0, int depth, int s, int *lo, int *hi) {
+  int l = lo0, h = hi0;
+  for (int t = depth - 1; t >= 0; --t) {
+    const int mid = (l + h) >> 1;
+    if ((s >> t) & 1)
+      l = mid + 1;
+    else
+      h = mid;
+  }
+  *lo = l;
+  *hi = h;
+}
+
+// Sub-node (and its range) `depth` levels below [lo0, hi0] that holds position p.
+__device__ __forceinline__ int sub_of(int lo0, int hi0, int depth, int p, int *lo, int *hi) {
+  int l = lo0, h = hi0, s = 0;
+  for (int t = 0; t < depth; ++t) {
+    const int mid = (l + h) >> 1;
+    if (p <= mid) {
+      h = mid;
+      s = 2 * s;
+    } else {
+      l = mid + 1;
+      s = 2 * s + 1;
+    }
+  }
+  *lo = l;
+  *hi = h;
+  return s;
+}
+
+__global__ void __launch_bounds__(kStThreads)
+    subtree_kernel(int L0, int ml, int N, const double *__restrict__ pos, const uint32_t *__restrict__ lists,
+                   int *__restrict__ lohi, const double *__restrict__ consts, double *__restrict__ bbox,
+                   int *__restrict__ argext, uint32_t *__restrict__ perm, int *__restrict__ lid,
+                   int *__restrict__ status) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  uint16_t *Lbuf = (uint16_t *)smem;                             // [2][3][kStCap] local ids
+  uint32_t *gid = (uint32_t *)(smem + 2 * 3 * kStCap * 2);       // local id -> particle id
+  int *scan = (int *)(gid + kStCap);                             // left flags before each position
+  uint8_t *flag = (uint8_t *)(scan + kStCap);                    // left flag per local id
+  __shared__ int s_warp[33];
+  __shared__ int s_split[kStMaxSub], s_mid[kStMaxSub];
+  const int tid = threadIdx.x;
+  const int k0 = (1 << L0) - 1 + blockIdx.x;
+  const int lo0 = lohi[2 * k0], hi0 = lohi[2 * k0 + 1], cnt = hi0 - lo0 + 1;
+  if (cnt < 1 || cnt > kStCap || ml - L0 > 10) {  // excluded by the host's choice of L0
+    if (tid == 0) atomicExch(status, kDevBadIndex);
+    return;
+  }
+  auto L = [&](int buf, int a) { return Lbuf + (buf * 3 + a) * kStCap; };
+  for (int j = tid; j < cnt; j += kStThreads) {
+    const uint32_t p = lists[lo0 + j];
+    gid[j] = p;
+    lid[p] = j;
+  }
+  __syncthreads();
+  for (int j = tid; j < cnt; j += kStThreads) {
+    L(0, 0)[j] = (uint16_t)j;
+    L(0, 1)[j] = (uint16_t)lid[lists[(int64_t)N + lo0 + j]];
+    L(0, 2)[j] = (uint16_t)lid[lists[2 * (int64_t)N + lo0 + j]];
+  }
+  __syncthreads();
+  int cur = 0;
+  for (int l = L0; l <= ml; ++l) {
+    const int depth = l - L0, nsub = 1 << depth;
+    for (int s = tid; s < nsub; s += kStThreads) {
+      int lo, hi;
+      sub_range(lo0, hi0, depth, s, &lo, &hi);
+      const int64_t k = ((int64_t)1 << l) - 1 + (int64_t)blockIdx.x * nsub + s;
+      lohi[2 * k] = lo;
+      lohi[2 * k + 1] = hi;
+      double bmin[3], bmax[3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        const uint32_t pmin = gid[L(cur, d)[lo - lo0]], pmax = gid[L(cur, d)[hi - lo0]];
+        bmin[d] = pos[3 * (int64_t)pmin + d];
+        bmax[d] = pos[3 * (int64_t)pmax + d];
+        bbox[6 * k + d] = bmin[d];
+        bbox[6 * k + 3 + d] = bmax[d];
+        argext[6 * k + d] = (int)pmin;
+        argext[6 * k + 3 + d] = (int)pmax;
+      }
+      if (l < ml) {
+        // splitdir = argmax(stretch .* (bbox[2] - bbox[1])), first maximum
+        const double v0 = rn_mul(consts[3], rn_sub(bmax[0], bmin[0]));
+        const double v1 = rn_mul(consts[4], rn_sub(bmax[1], bmin[1]));
+        const double v2 = rn_mul(consts[5], rn_sub(bmax[2], bmin[2]));
+        int dir = 0;
+        double best = v0;
+        if (v1 > best) {
+          best = v1;
+          dir = 1;
+        }
+        if (v2 > best) dir = 2;
+        s_split[s] = dir;
+        s_mid[s] = (lo + hi) >> 1;
+      }
+    }
+    __syncthreads();
+    if (l == ml) break;
+    // left flags: the first ceil(cnt/2) of each node's split-axis segment
+    for (int p = tid; p < cnt; p += kStThreads) {
+      int lo, hi;
+      const int s = sub_of(lo0, hi0, depth, lo0 + p, &lo, &hi);
+      flag[L(cur, s_split[s])[p]] = (lo0 + p <= s_mid[s]) ? 1 : 0;
+    }
+    __syncthreads();
+    for (int a = 0; a < 3; ++a) {
+      const int b0 = tid * kStItems;
+      uint8_t f[kStItems];
+      int c = 0;
+#pragma unroll
+      for (int i = 0; i < kStItems; ++i) {
+        const int p = b0 + i;
+        f[i] = p < cnt ? flag[L(cur, a)[p]] : 0;
+        c += f[i];
+      }
+      int ex = block_excl_scan(c, s_warp, nullptr);
+#pragma unroll
+      for (int i = 0; i < kStItems; ++i) {
+        const int p = b0 + i;
+        if (p < cnt) scan[p] = ex;
+        ex += f[i];
+      }
+      __syncthreads();
+#pragma unroll
+      for (int i = 0; i < kStItems; ++i) {
+        const int p = b0 + i;
+        if (p < cnt) {
+          int lo, hi;
+          const int s = sub_of(lo0, hi0, depth, lo0 + p, &lo, &hi);
+          const int lb = scan[p] - scan[lo - lo0];  // left flags before p inside its node
+          const int dest = f[i] ? lo + lb : s_mid[s] + 1 + ((lo0 + p - lo) - lb);
+          if (dest < lo || dest > hi)  // stays inside the node by construction
+            atomicExch(status, kDevBadIndex);
+          else
+            L(cur ^ 1, a)[dest - lo0] = L(cur, a)[p];
+        }
+      }
+      __syncthreads();
+    }
+    cur ^= 1;
+  }
+  // leaves: particle ids in ascending order
+  uint32_t *vals = (uint32_t *)scan;
+  for (int p = tid; p < cnt; p += kStThreads) vals[p] = gid[L(cur, 0)[p]];
+  __syncthreads();
+  const int depth = ml - L0;
+  for (int p = tid; p < cnt; p += kStThreads) {
+    int lo, hi;
+    sub_of(lo0, hi0, depth, lo0 + p, &lo, &hi);
+    const uint32_t v = vals[p];
+    int r = 0;
+    for (int q = lo - lo0; q <= hi - lo0; ++q) r += vals[q] < v ? 1 : 0;
+    perm[lo + r] = v;
+  }
+}
+
 // Leaf-local FP32 records: coordinates relative to the leaf's box centre.
 __global__ void gather32_kernel(int ml, int N, const uint32_t *__restrict__ perm,
                                 const double *__restrict__ pos, const double *__restrict__ mom,
@@ -502,10 +678,16 @@ int build_tree(Ctx *ctx, const double *d_pos, int64_t N64, int64_t N0, const dou
     FMM_CUDA_TRY(ctx, cudaMemcpyAsync(lists + (int64_t)a * N, alt ? vB : vA, sizeof(uint32_t) * N,
                                       cudaMemcpyDeviceToDevice, ctx->stream));
   }
-  // 2. levels
+  // 2. levels: globally down to L0, the first level whose nodes fit one CTA (and at
+  // most 10 levels above the leaves), then each level-L0 subtree in shared memory
+  int L0 = 0;
+  while (L0 < ml && (((N64 + ((int64_t)1 << L0) - 1) >> L0) > kStCap || ml - L0 > 10)) ++L0;
+  // leaves larger than one CTA (N0 > kStCap): every level globally, then the sort by leaf
+  const bool subtree = ((N64 + ((int64_t)1 << L0) - 1) >> L0) <= kStCap;
+  if (!subtree) L0 = ml + 1;
   int root[2] = {0, N - 1};
   FMM_CUDA_TRY(ctx, cudaMemcpyAsync(lohi, root, sizeof(root), cudaMemcpyHostToDevice, ctx->stream));
-  for (int l = 0; l <= ml; ++l) {
+  for (int l = 0; l < L0; ++l) {
     const int cnt_level = 1 << l;
     node_kernel<<<ceil_div(cnt_level, TB), TB, 0, ctx->stream>>>(l, ml, N, d_pos, lists, lohi, d_consts, bbox,
                                                                   argext, split, half);
@@ -525,12 +707,22 @@ int build_tree(Ctx *ctx, const double *d_pos, int64_t N64, int64_t N0, const dou
   }
   // the buffers may have swapped roles: keep names consistent for later stages
   if (lists != ctx->get<uint32_t>("lists")) std::swap(ctx->bufs["lists"], ctx->bufs["lists_next"]);
-  // 3. canonical order: particle ids ascending inside each leaf
-  leafof_kernel<<<ceil_div(N, TB), TB, 0, ctx->stream>>>(ml, N, lists, kA, vA);
-  FMM_TRY(ctx->check_launch("leafof_kernel"));
-  bool alt = false;
-  FMM_TRY(radix_sort(ctx, kA, kB, vA, vB, N, ml, &alt));
-  FMM_CUDA_TRY(ctx, cudaMemcpyAsync(perm, alt ? vB : vA, sizeof(uint32_t) * N, cudaMemcpyDeviceToDevice, ctx->stream));
+  // 3. levels L0 .. ml and the canonical order (particle ids ascending inside each leaf)
+  if (subtree) {
+    int *lid;
+    FMM_TRY(ctx->ensure("tree_lid", N, &lid));
+    FMM_TRY(opt_in_smem(ctx, subtree_kernel, kStSmem));
+    subtree_kernel<<<1u << L0, kStThreads, kStSmem, ctx->stream>>>(L0, ml, N, d_pos, lists, lohi, d_consts, bbox,
+                                                                    argext, perm, lid, ctx->d_status);
+    FMM_TRY(ctx->check_launch("subtree_kernel"));
+  } else {
+    leafof_kernel<<<ceil_div(N, TB), TB, 0, ctx->stream>>>(ml, N, lists, kA, vA);
+    FMM_TRY(ctx->check_launch("leafof_kernel"));
+    bool alt = false;
+    FMM_TRY(radix_sort(ctx, kA, kB, vA, vB, N, ml, &alt));
+    FMM_CUDA_TRY(ctx, cudaMemcpyAsync(perm, alt ? vB : vA, sizeof(uint32_t) * N, cudaMemcpyDeviceToDevice,
+                                      ctx->stream));
+  }
 
   ctx->N = N;
   ctx->N0 = N0;

@@ -38,7 +38,8 @@ def make(kind, N, seed):
 
 # ------------------------------------------------------------------------- tree
 @pytest.mark.parametrize("N,N0,kind", [(10000, 32, "uniform"), (65536, 125, "gauss"), (100003, 50, "beamlets"),
-                                       (1000, 400, "uniform"), (100, 200, "uniform"), (1, 5, "uniform")])
+                                       (1000, 400, "uniform"), (100, 200, "uniform"), (1, 5, "uniform"),
+                                       (20000, 5000, "gauss"), (100000, 2, "uniform"), (300000, 100, "gauss")])
 def test_cluster_tree_bit_exact(gpu_ctx, oracle_mod, N, N0, kind):
     pos, mom = make(kind, N, 3)
     stretch = oracle_mod.stretch(oracle_mod.pavg(mom))
