@@ -12,6 +12,9 @@ tree build, traversal, P2M/M2M, M2L, P2P, L2L/L2P.
            makes): pinned host inputs copied in and fields copied out every step
   fwd_bwd  one forward (saving its state) plus the hand-written adjoint of
            L = sum(w.E + v.B) back to positions and momenta, device-resident
+  reuse    a drifting beam (x += 1e-12 u between calls, outside the timed region)
+           evaluated with fmmb200_set_tree_reuse: the forward keeps the tree when
+           a rebuild would give the same one (checked exactly on the device)
   roofline the dominant kernel (M2L) against the measured CUDA-core FMA peak
   accuracy rel-L2 of mixed vs FP64 over all particles, and of both vs an FP64
            direct sum (GPU) on 4096 seeded targets
@@ -67,6 +70,7 @@ def parse():
     ap.add_argument("--skip-cpu-baseline", action="store_true")
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-backward", action="store_true")
+    ap.add_argument("--skip-reuse", action="store_true")
     ap.add_argument("--m2l-engine", choices=["auto", "cuda_cores", "tensor_cores"], default="auto",
                     help="mixed-form M2L engine (fmmb200_set_m2l_engine)")
     ap.add_argument("--bwd-steps", type=int, default=3, help="timed fwd+bwd steps (after 2 warm-up steps)")
@@ -347,6 +351,31 @@ def run_ours(args, world, rank, local):
                              "unit": "particles/s", "ratio_to_forward": ms_fb / ms_f, "steps": args.bwd_steps,
                              "warmup": 2, "grad_finite": bool(torch.isfinite(gx).all() and torch.isfinite(gu).all())}
 
+    # tree reuse on a slowly drifting beam (mixed form)
+    reuse = None
+    if not args.skip_reuse:
+        posd = pos.clone()
+        ctx.set_tree_reuse(True)
+        step(alg_mixed, E, B)  # builds the tree this loop starts from
+        step(alg_mixed, E, B)
+        stream.synchronize()
+        total, kept = 0.0, 0
+        for _ in range(args.steps):
+            posd.add_(mom, alpha=1e-12)
+            torch.cuda.synchronize(dev)
+            ev0 = torch.cuda.Event(enable_timing=True)
+            ev1 = torch.cuda.Event(enable_timing=True)
+            ev0.record(stream)
+            ctx.forward_device(N, posd.data_ptr(), mom.data_ptr(), E.data_ptr(), B.data_ptr(), alg_mixed)
+            ev1.record(stream)
+            ev1.synchronize()
+            total += ev0.elapsed_time(ev1)
+            kept += int(ctx.stats()["tree_reused"])
+        ctx.set_tree_reuse(False)
+        ms_r = max_over_ranks(world, total / args.steps)
+        reuse = {"ms_per_step": ms_r, "value": replicas.aggregate_rate(world, N, ms_r), "unit": "particles/s",
+                 "steps": args.steps, "steps_tree_kept": kept, "ms_tree_last": ctx.stats()["ms_tree"]}
+
     # roofline of the dominant kernel (M2L) against the measured CUDA-core FMA peak
     p64 = ctypes.c_double()
     p32 = ctypes.c_double()
@@ -426,6 +455,7 @@ def run_ours(args, world, rank, local):
                      "device_bytes_with_backward": bwd_bytes,
                      "torch_peak_bytes": int(torch.cuda.max_memory_allocated(dev))},
             "fwd_bwd": fwd_bwd,
+            "reuse": reuse,
             "roofline": roof,
             "cpu_baseline": cpu,
             "e2e": e2e,

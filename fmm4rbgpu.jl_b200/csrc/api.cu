@@ -119,7 +119,9 @@ int run_forward(Ctx *ctx, int64_t N, const double *d_pos, const double *d_mom, d
     FMM_TRY(compute_pavg_stretch(ctx, d_mom, N, consts));
   }
   ctx->pavg_from_momenta = pavg_host == nullptr;
-  FMM_TRY(build_tree(ctx, d_pos, N, N0, consts));
+  bool reused = false;
+  if (ctx->tree_reuse) FMM_TRY(refit_tree(ctx, d_pos, N, N0, consts, &reused));
+  if (!reused) FMM_TRY(build_tree(ctx, d_pos, N, N0, consts));
   FMM_TRY(gather_particles(ctx, d_pos, d_mom, mixed));
   FMM_TRY(compute_nodes(ctx, n));
   ctx->n = n;
@@ -184,6 +186,7 @@ int run_forward(Ctx *ctx, int64_t N, const double *d_pos, const double *d_mom, d
   const double NN = (double)(n + 1) * (n + 1) * (n + 1);
   st.m2l_kernel_evals = (double)ctx->nm2l * NN * NN;
   st.kernel_launches = ctx->launches - launches0;
+  st.tree_reused = reused ? 1 : 0;
   st.p2p_kernel_evals = p2p_evals;
   if (ctx->timing) {
     st.ms_tree = ev_ms(ctx, kEvH2D, kEvTree);
@@ -428,6 +431,12 @@ int fmmb200_set_timing(fmmb200_ctx *ctx, int enable) {
 int fmmb200_set_m2l_engine(fmmb200_ctx *ctx, int engine) {
   if (!ctx || engine < FMMB200_M2L_AUTO || engine > FMMB200_M2L_TENSOR_CORES) return FMMB200_ERR_INVALID_ARGUMENT;
   ctx->m2l_engine = engine;
+  return FMMB200_OK;
+}
+
+int fmmb200_set_tree_reuse(fmmb200_ctx *ctx, int enable) {
+  if (!ctx) return FMMB200_ERR_INVALID_ARGUMENT;
+  ctx->tree_reuse = enable != 0;
   return FMMB200_OK;
 }
 

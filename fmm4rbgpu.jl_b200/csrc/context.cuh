@@ -46,6 +46,7 @@ struct fmmb200_ctx {
   int traversal_steps = 0;
   int list_bits = 1;  // pair keys are (target << list_bits) | source
   int m2l_engine = 0;  // FMMB200_M2L_*: mixed-form M2L engine
+  bool tree_reuse = false;  // forward: refit the previous tree when it is still exact
   fmmb200_stats stats{};
 
   // pairwise-summation plan for p_avg (depends on N only)

@@ -31,6 +31,11 @@ int compute_pavg_stretch(Ctx *ctx, const double *d_mom_aos, int64_t N, double *d
 // Build the cluster tree of N particles (AoS positions on device) with the
 // stretch in d_consts[3..5]; fills ctx tree buffers and ctx->{N,N0,ml,nc,...}.
 int build_tree(Ctx *ctx, const double *d_pos_aos, int64_t N, int64_t N0, const double *d_consts);
+// Refit the existing tree (same N, N0) to new positions: boxes and extremal
+// particles bottom-up, and *same = true when every node would split as before, in
+// which case the tree equals what build_tree would give.  Otherwise the refitted
+// boxes are garbage and the caller rebuilds.
+int refit_tree(Ctx *ctx, const double *d_pos_aos, int64_t N, int64_t N0, const double *d_consts, bool *same);
 // Particle records in tree order ("prec64": x,y,z,gamma,ux,uy,uz,0) and, for
 // the mixed form, leaf-local FP32 records ("prec32": x,y,z,gamma,ux,uy,uz,0
 // relative to the leaf's box centre) and the P2P source records ("prec32x2":

@@ -493,6 +493,91 @@ __global__ void __launch_bounds__(kStThreads)
   }
 }
 
+// ---------------------------------------------------------------- refit of an existing tree
+// For a tree of the same N and N0 (same node ranges), new positions give the same
+// tree exactly when every internal node still splits its particles the same way:
+// with the boxes refitted bottom-up (exact min/max; the extremal particle is the
+// first / last in (coordinate, id) order, as the sorted segment ends give it), the
+// node's split axis argmax(stretch .* extent) must leave the left child's last
+// particle before the right child's first in (coordinate, id) order.  Then the
+// permutation, boxes and extremal particles equal what build_tree would compute.
+__device__ __forceinline__ bool lex_less(double a, int ia, double b, int ib) {
+  return a < b || (a == b && ia < ib);
+}
+
+__global__ void refit_leaf_kernel(int64_t leaf0, int64_t nleaf, const int *__restrict__ lohi,
+                                  const uint32_t *__restrict__ perm, const double *__restrict__ pos,
+                                  double *__restrict__ bbox, int *__restrict__ argext) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nleaf) return;
+  const int64_t c = leaf0 + i;
+  const int lo = lohi[2 * c], hi = lohi[2 * c + 1];
+  double vmin[3], vmax[3];
+  int imin[3], imax[3];
+  {
+    const int p = (int)perm[lo];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      vmin[d] = vmax[d] = pos[3 * (int64_t)p + d];
+      imin[d] = imax[d] = p;
+    }
+  }
+  for (int j = lo + 1; j <= hi; ++j) {
+    const int p = (int)perm[j];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const double v = pos[3 * (int64_t)p + d];
+      if (lex_less(v, p, vmin[d], imin[d])) {
+        vmin[d] = v;
+        imin[d] = p;
+      }
+      if (lex_less(vmax[d], imax[d], v, p)) {
+        vmax[d] = v;
+        imax[d] = p;
+      }
+    }
+  }
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    bbox[6 * c + d] = vmin[d];
+    bbox[6 * c + 3 + d] = vmax[d];
+    argext[6 * c + d] = imin[d];
+    argext[6 * c + 3 + d] = imax[d];
+  }
+}
+
+__global__ void refit_up_kernel(int l, const double *__restrict__ consts, double *__restrict__ bbox,
+                                int *__restrict__ argext, int *__restrict__ changed) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= ((int64_t)1 << l)) return;
+  const int64_t k = ((int64_t)1 << l) - 1 + idx, a = 2 * k + 1, b = 2 * k + 2;
+  double lo[3], hi[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const bool la = lex_less(bbox[6 * a + d], argext[6 * a + d], bbox[6 * b + d], argext[6 * b + d]);
+    lo[d] = la ? bbox[6 * a + d] : bbox[6 * b + d];
+    argext[6 * k + d] = la ? argext[6 * a + d] : argext[6 * b + d];
+    const bool hb = lex_less(bbox[6 * a + 3 + d], argext[6 * a + 3 + d], bbox[6 * b + 3 + d], argext[6 * b + 3 + d]);
+    hi[d] = hb ? bbox[6 * b + 3 + d] : bbox[6 * a + 3 + d];
+    argext[6 * k + 3 + d] = hb ? argext[6 * b + 3 + d] : argext[6 * a + 3 + d];
+    bbox[6 * k + d] = lo[d];
+    bbox[6 * k + 3 + d] = hi[d];
+  }
+  // the split this node would get from the new positions (node_kernel's rule)
+  const double v0 = rn_mul(consts[3], rn_sub(hi[0], lo[0]));
+  const double v1 = rn_mul(consts[4], rn_sub(hi[1], lo[1]));
+  const double v2 = rn_mul(consts[5], rn_sub(hi[2], lo[2]));
+  int dir = 0;
+  double best = v0;
+  if (v1 > best) {
+    best = v1;
+    dir = 1;
+  }
+  if (v2 > best) dir = 2;
+  if (!lex_less(bbox[6 * a + 3 + dir], argext[6 * a + 3 + dir], bbox[6 * b + dir], argext[6 * b + dir]))
+    atomicOr(changed, 1);
+}
+
 // Leaf-local FP32 records: coordinates relative to the leaf's box centre.
 __global__ void gather32_kernel(int ml, int N, const uint32_t *__restrict__ perm,
                                 const double *__restrict__ pos, const double *__restrict__ mom,
@@ -732,6 +817,30 @@ int build_tree(Ctx *ctx, const double *d_pos, int64_t N64, int64_t N0, const dou
   ctx->leaf0 = leaf0;
   ctx->max_leaf = (N64 + ((int64_t)1 << ml) - 1) >> ml;
   ctx->have_tree = true;
+  return FMMB200_OK;
+}
+
+int refit_tree(Ctx *ctx, const double *d_pos, int64_t N, int64_t N0, const double *d_consts, bool *same) {
+  *same = false;
+  if (!ctx->have_tree || ctx->N != N || ctx->N0 != N0) return FMMB200_OK;
+  const int ml = ctx->ml;
+  int *changed, *h;
+  FMM_TRY(ctx->ensure("refit_flag", 1, &changed));
+  FMM_CUDA_TRY(ctx, cudaMemsetAsync(changed, 0, sizeof(int), ctx->stream));
+  double *bbox = ctx->get<double>("bbox");
+  int *argext = ctx->get<int>("argext");
+  refit_leaf_kernel<<<ceil_div(ctx->nleaf, 128), 128, 0, ctx->stream>>>(
+      ctx->leaf0, ctx->nleaf, ctx->get<int>("lohi"), ctx->get<uint32_t>("perm"), d_pos, bbox, argext);
+  FMM_TRY(ctx->check_launch("refit_leaf_kernel"));
+  for (int l = ml - 1; l >= 0; --l) {
+    refit_up_kernel<<<ceil_div(1 << l, 256), 256, 0, ctx->stream>>>(l, d_consts, bbox, argext, changed);
+    FMM_TRY(ctx->check_launch("refit_up_kernel"));
+  }
+  FMM_TRY(ctx->pinned(sizeof(int), (void **)&h));
+  FMM_CUDA_TRY(ctx, cudaMemcpyAsync(h, changed, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  FMM_TRY(ctx->sync());
+  *same = h[0] == 0;
+  ctx->have_lists = ctx->have_forward = ctx->saved = false;
   return FMMB200_OK;
 }
 

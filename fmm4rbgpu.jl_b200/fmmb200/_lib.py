@@ -56,6 +56,7 @@ class Stats(ctypes.Structure):
         ("ms_h2d", c_f64), ("ms_tree", c_f64), ("ms_lists", c_f64), ("ms_upward", c_f64), ("ms_m2l", c_f64),
         ("ms_p2p", c_f64), ("ms_downward", c_f64), ("ms_d2h", c_f64), ("ms_total", c_f64), ("ms_backward", c_f64),
         ("m2l_kernel_evals", c_f64), ("p2p_kernel_evals", c_f64), ("kernel_launches", c_i64),
+        ("tree_reused", c_i64),
     ]
 
     def as_dict(self) -> dict:
@@ -105,6 +106,7 @@ SIGNATURES = {
     "fmmb200_direct_device": (ctypes.c_int, [c_vp, c_i64, c_vp, c_vp, c_f64, c_f64, c_i64, c_vp, c_vp, c_vp]),
     "fmmb200_measure_fma_peak": (ctypes.c_int, [c_vp, p_f64, p_f64, p_f64]),
     "fmmb200_set_m2l_engine": (ctypes.c_int, [c_vp, ctypes.c_int]),
+    "fmmb200_set_tree_reuse": (ctypes.c_int, [c_vp, ctypes.c_int]),
     "fmmb200_direct_noalloc": (ctypes.c_int, [c_i64, c_vp, c_vp, c_f64, c_f64, c_i64, c_vp, c_vp, c_vp, c_vp]),
 }
 

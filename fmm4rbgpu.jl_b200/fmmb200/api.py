@@ -152,6 +152,11 @@ class Context:
             raise ValueError(f"engine must be one of {sorted(codes)}")
         self._check(self._lib.fmmb200_set_m2l_engine(self._h, codes[engine]))
 
+    def set_tree_reuse(self, enable: bool):
+        """Keep the previous tree when new positions would split every node the same
+        way (checked exactly on the device); see fmmb200_set_tree_reuse."""
+        self._check(self._lib.fmmb200_set_tree_reuse(self._h, int(bool(enable))))
+
     def debug_fail_alloc(self, k: int):
         self._check(self._lib.fmmb200_debug_fail_alloc(self._h, int(k)))
 

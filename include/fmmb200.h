@@ -63,6 +63,7 @@ typedef struct fmmb200_stats {
   double m2l_kernel_evals; /* sum over M2L pairs of (n+1)^6 */
   double p2p_kernel_evals; /* sum over P2P pairs of |t|*|s| */
   int64_t kernel_launches; /* CUDA kernels launched by the last forward */
+  int64_t tree_reused;     /* 1 if the last forward refitted the previous tree (fmmb200_set_tree_reuse) */
 } fmmb200_stats;
 
 /* ---- lifecycle ------------------------------------------------------------ */
@@ -84,6 +85,15 @@ int fmmb200_set_timing(fmmb200_ctx *ctx, int enable);
 #define FMMB200_M2L_CUDA_CORES 1
 #define FMMB200_M2L_TENSOR_CORES 2
 int fmmb200_set_m2l_engine(fmmb200_ctx *ctx, int engine);
+/* Tree reuse across calls (no counterpart in the reference, which rebuilds the tree on
+ * the host every call).  When enabled and the next forward has the same npar and N0 as
+ * the previous tree, the library refits the boxes to the new positions and checks on
+ * the device that every node would split its particles exactly as before (same split
+ * axis, the left half still before the right half in coordinate-then-id order).  If so
+ * the tree is kept -- it is bit-identical to a rebuild, so the fields are the same --
+ * and the radix sorts and partitions are skipped; otherwise the tree is rebuilt.  For
+ * time-stepping loops whose particles move little per step.  Off by default. */
+int fmmb200_set_tree_reuse(fmmb200_ctx *ctx, int enable);
 /* Fault injection for tests: the k-th next device allocation fails (k >= 1; 0 disables). */
 int fmmb200_debug_fail_alloc(fmmb200_ctx *ctx, int64_t k);
 

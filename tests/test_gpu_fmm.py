@@ -274,3 +274,44 @@ def test_tree_and_lists_after_forward_match_oracle(gpu_ctx, oracle_mod):
     rp2p, rm2l = oracle_mod.interaction_lists(ref["children"], ref["bboxes"], stretch, 0.5)
     np.testing.assert_array_equal(m2l, rm2l[np.lexsort((rm2l[:, 1], rm2l[:, 0]))])
     np.testing.assert_array_equal(p2p, rp2p[np.lexsort((rp2p[:, 1], rp2p[:, 0]))])
+
+
+def test_tree_reuse_is_exact(gpu_ctx):
+    """fmmb200_set_tree_reuse: the refitted tree is kept only when a rebuild would give
+    the same tree, so fields, tree and lists are bit-identical to a fresh build."""
+    import fmmb200
+
+    pos, mom = make("gauss", 50000, 6)
+    alg = fmmb200.FMMB200(n=4, N0=64, eta=0.5)
+    fresh = fmmb200.Context(0)
+    try:
+        gpu_ctx.set_tree_reuse(True)
+        gpu_ctx.forward(pos, mom, alg)
+        assert gpu_ctx.stats()["tree_reused"] == 0  # nothing to reuse on the first call of this size
+        E1, B1 = gpu_ctx.forward(pos, mom, alg)  # same positions
+        assert gpu_ctx.stats()["tree_reused"] == 1
+        Ef, Bf = fresh.forward(pos, mom, alg)
+        assert np.array_equal(E1, Ef) and np.array_equal(B1, Bf)
+        # a small drift: same splits, new boxes and fields
+        pos2 = pos + 1e-9 * np.random.default_rng(1).normal(size=pos.shape)
+        E2, B2 = gpu_ctx.forward(pos2, mom, alg)
+        assert gpu_ctx.stats()["tree_reused"] == 1
+        Ef, Bf = fresh.forward(pos2, mom, alg)
+        assert np.array_equal(E2, Ef) and np.array_equal(B2, Bf)
+        t, tf = gpu_ctx.tree(), fresh.tree()
+        for key in ("parindices", "parlohis", "bboxes"):
+            assert np.array_equal(t[key], tf[key]), key
+        m, p = gpu_ctx.lists()
+        mf, pf = fresh.lists()
+        assert np.array_equal(m, mf) and np.array_equal(p, pf)
+        # new positions that change the splits: rebuilt
+        pos3, mom3 = make("gauss", 50000, 7)
+        E3, _ = gpu_ctx.forward(pos3, mom3, alg)
+        assert gpu_ctx.stats()["tree_reused"] == 0
+        assert np.array_equal(E3, fresh.forward(pos3, mom3, alg)[0])
+        # another size: rebuilt
+        gpu_ctx.forward(pos3[:40000], mom3[:40000], alg)
+        assert gpu_ctx.stats()["tree_reused"] == 0
+    finally:
+        gpu_ctx.set_tree_reuse(False)
+        fresh.close()
