@@ -855,6 +855,258 @@ __global__ void __launch_bounds__(MBShape2<NDEG>::BT)
   if (tid < 3) gp_part[3 * (int64_t)t + tid] = gpv[tid];
 }
 
+// M2L^T, mixed form, eta <= 1/2 (no two nodes of a pair coincide): one own node per
+// thread in scalar FP32, the sums over the source nodes b factored so that every term
+// linear in the source data costs one FMA per evaluation.  With R = x_a - y_b (both
+// relative to the cluster's own centre) and f = s^3, f5 = s^5, s = d^{-1/2}:
+//   sum f c          = gE_a SfG + gB_a x SfM - Gamma_a SfE + M_a x SfH
+//   sum f R.gE_b     = x_a . SfE - Sfe,     sum f R x gB_b = x_a x SfH - Sfh
+// where SfG = sum f Gamma_b, SfM = sum f M_b, SfE = sum f gE_b, SfH = sum f gB_b,
+// Sfe = sum f (y_b . gE_b) and Sfh = sum f (y_b x gB_b); the last two are packed with
+// the source data.  The scalar
+//   R.c = Gamma_b (R.gE_a) + M_b.(R x gB_a) - Gamma_a (R.gE_b) + gB_b.(R x M_a)
+// takes the parts of R.gE_a, R x gB_a and R x M_a that do not depend on the source
+// column from the row and plane loops.  Per source pair the FP32 sums are combined
+// into ten per-node values (node gradient, Gamma and M adjoints, p_avg partial) and
+// added into FP64 sums in shared memory.  Scalar rather than packed FP32x2: the 21
+// running sums of two nodes per thread would not fit the register file.
+template <int NDEG>
+struct MBShape1F {
+  static constexpr int M = NDEG + 1;
+  static constexpr int NN = M * M * M;
+  static constexpr int NS = ((3 * M) + 1) & ~1;
+  static constexpr int BT = ((NN + 31) / 32) * 32;
+  static constexpr int RECF = MBShape2<NDEG>::RECF;  // the staged records of m2l_bwd_x2_kernel
+  static constexpr int RAWB = RECF * 4;
+  static constexpr int REC = RAWB + NS * 8;
+  static constexpr int PKV = 4;   // float4 per packed source node
+  static constexpr int NF = 10;   // FP64 sums per node: gx(3) gGamma gM(3) gp(3)
+  static constexpr int SMEM = 2 * REC + PKV * NN * 16 + NF * BT * 8;
+  // resident CTAs asked of the register allocator: 512 threads per SM, i.e. at most
+  // 128 registers per thread (n = 4: four CTAs of 128 threads; measured 5 % faster
+  // than the unbounded 167-register build)
+  static constexpr int MINB = BT >= 512 ? 1 : 512 / BT;
+};
+
+template <int NDEG>
+__global__ void __launch_bounds__(MBShape1F<NDEG>::BT, MBShape1F<NDEG>::MINB)
+    m2l_bwd_x1f_kernel(const int *__restrict__ ptr, const int *__restrict__ src, const uint8_t *__restrict__ flg,
+                       const double *__restrict__ nodes, const double *__restrict__ bbox, ChebT ct,
+                       const float *__restrict__ rec32, const double *__restrict__ consts, double *__restrict__ gmom,
+                       double *__restrict__ gbox, double *__restrict__ gp_part, int *__restrict__ status) {
+  using S = MBShape1F<NDEG>;
+  constexpr int M = S::M, NN = S::NN, NS = S::NS, BT = S::BT, RECF = S::RECF, RAWB = S::RAWB;
+  constexpr int REC = S::REC, NF = S::NF, PKV = S::PKV;
+  extern __shared__ __align__(16) unsigned char smem[];
+  float4 *pk = (float4 *)(smem + 2 * REC);                      // PKV NN packed per-node operands
+  double *s_acc = (double *)(smem + 2 * REC + PKV * NN * 16);    // [NF][BT] FP64 sums
+  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ double s_sn[3 * M];  // source node offsets from the own centre
+  __shared__ double s_red[32 * 6];
+  __shared__ double s_ct[M];
+
+  const int tid = threadIdx.x;
+  const int t = blockIdx.x;
+  if (tid == 0) {
+#pragma unroll
+    for (int i = 0; i < M; ++i) s_ct[i] = ct.t[i];
+  }
+  const int p0 = ptr[t], np = ptr[t + 1] - p0;
+  const double *tn = nodes + (int64_t)t * NS;
+  const double *tb = bbox + 6 * (int64_t)t;
+  const double cx = 0.5 * (tb[0] + tb[3]), cy = 0.5 * (tb[1] + tb[4]), cz = 0.5 * (tb[2] + tb[5]);
+  const bool act = tid < NN;
+  const int a = act ? tid : 0;
+  const double tx = tn[a % M] - cx, ty = tn[M + (a / M) % M] - cy, tz = tn[2 * M + a / (M * M)] - cz;
+  const float *own = rec32 + (int64_t)t * RECF;
+  const float Ga = own[a], Ma0 = own[NN + a], Ma1 = own[2 * NN + a], Ma2 = own[3 * NN + a];
+  const float gE0 = own[4 * NN + a], gE1 = own[5 * NN + a], gE2 = own[6 * NN + a];
+  const float gB0 = own[7 * NN + a], gB1 = own[8 * NN + a], gB2 = own[9 * NN + a];
+  for (int q = 0; q < NF; ++q) s_acc[q * BT + tid] = 0.0;
+  const float py = (float)consts[1], pz = (float)consts[2];
+  const float eps = (float)kEps64;
+
+  if (np > 0) {
+    if (tid == 0) {
+      mbar_init(&bar[0], 1);
+      mbar_init(&bar[1], 1);
+      fence_mbar_init();
+    }
+    __syncthreads();
+    auto issue = [&](int k, int bb) {
+      const int s = src[p0 + k];
+      unsigned char *dst = smem + bb * REC;
+      mbar_arrive_expect_tx(&bar[bb], REC);
+      bulk_g2s(dst, rec32 + (int64_t)s * RECF, RAWB, &bar[bb]);
+      bulk_g2s(dst + RAWB, nodes + (int64_t)s * NS, NS * 8, &bar[bb]);
+    };
+    if (tid == 0) issue(0, 0);
+    for (int i = 0; i < np; ++i) {
+      const int bb = i & 1;
+      const int fl = flg[p0 + i];
+      if (tid == 0 && i + 1 < np) {
+        fence_proxy_async_smem();
+        issue(i + 1, bb ^ 1);
+      }
+      const bool ok = mbar_wait_bounded(&bar[bb], (uint32_t)((i >> 1) & 1), status);
+      const float *G = (const float *)(smem + bb * REC);
+      const double *SN = (const double *)(smem + bb * REC + RAWB);
+      if (ok) {
+        for (int e = tid; e < 3 * M; e += BT) {
+          const int d = e / M;
+          s_sn[e] = SN[e] - (d == 0 ? cx : (d == 1 ? cy : cz));
+        }
+        // A pair in only one role zeroes the other role's half of the source data.
+        const float k1 = (fl & 1) ? 1.f : 0.f, k2 = (fl & 2) ? 1.f : 0.f;
+        for (int b = tid; b < NN; b += BT) {
+          float v[10];
+#pragma unroll
+          for (int q = 0; q < 10; ++q) v[q] = G[q * NN + b] * (q < 4 ? k1 : k2);
+          const double yx = SN[b % M] - cx, yy = SN[M + (b / M) % M] - cy, yz = SN[2 * M + b / (M * M)] - cz;
+          const float e = (float)(yx * v[4] + yy * v[5] + yz * v[6]);
+          const float h0 = (float)(yy * v[9] - yz * v[8]), h1 = (float)(yz * v[7] - yx * v[9]),
+                      h2 = (float)(yx * v[8] - yy * v[7]);
+          float4 *o = pk + PKV * b;
+          o[0] = make_float4(v[0], v[1], v[2], v[3]);  // Gamma, M
+          o[1] = make_float4(v[4], v[5], v[6], v[7]);  // gE, gB0
+          o[2] = make_float4(v[8], v[9], e, h0);       // gB1, gB2, y.gE, (y x gB)0
+          o[3] = make_float4(h1, h2, 0.f, 0.f);        // (y x gB)1, (y x gB)2
+        }
+      }
+      __syncthreads();
+      if (ok && act && fl != 0) {
+        float rxv[M], prx[M], rx2[M], ryv[M];
+        {
+          const float px = (float)consts[0];
+#pragma unroll
+          for (int b = 0; b < M; ++b) {
+            const float rx = (float)(tx - s_sn[b]);
+            rxv[b] = rx;
+            prx[b] = px * rx;
+            rx2[b] = rx * rx;
+            ryv[b] = (float)(ty - s_sn[M + b]);
+          }
+        }
+        float SfG = 0.f, SfM0 = 0.f, SfM1 = 0.f, SfM2 = 0.f, SfE0 = 0.f, SfE1 = 0.f, SfE2 = 0.f;
+        float SfH0 = 0.f, SfH1 = 0.f, SfH2 = 0.f, Sfe = 0.f, Sfh0 = 0.f, Sfh1 = 0.f, Sfh2 = 0.f;
+        float aw0 = 0.f, aw1 = 0.f, aw2 = 0.f, sp = 0.f, ap0 = 0.f, ap1 = 0.f, ap2 = 0.f;
+#pragma unroll 1
+        for (int bk = 0; bk < M; ++bk) {
+          const float rz = (float)(tz - s_sn[2 * M + bk]);
+          const float prz = pz * rz;
+          const float rzz = fmaf(rz, rz, eps);
+          const float ek = rz * gE2;   // (R.gE_a): z part
+          const float w1k = rz * gB0;  // (R x gB_a)_1 = rz gB0 - rx gB2
+          const float v1k = rz * Ma0;  // (R x M_a)_1 = rz Ma0 - rx Ma2
+#pragma unroll
+          for (int bj = 0; bj < M; ++bj) {
+            const float ry = ryv[bj];
+            const float P = fmaf(py, ry, prz);
+            const float A = fmaf(ry, ry, rzz);
+            const float ejk = fmaf(ry, gE1, ek);
+            const float w0 = fmaf(ry, gB2, -(rz * gB1));  // (R x gB_a)_0
+            const float w2j = -(ry * gB0);                // (R x gB_a)_2 = rx gB1 - ry gB0
+            const float v0 = fmaf(ry, Ma2, -(rz * Ma1));  // (R x M_a)_0
+            const float v2j = -(ry * Ma0);                // (R x M_a)_2 = rx Ma1 - ry Ma0
+            const float4 *pb = pk + PKV * M * (bj + M * bk);
+#pragma unroll
+            for (int bi = 0; bi < M; ++bi) {
+              const float rx = rxv[bi];
+              const float tt = P + prx[bi];  // p.R
+              const float d = fmaf(tt, tt, A + rx2[bi]);
+              const float sv = rsqrt_approx_f32(d);
+              const float s2 = sv * sv;
+              const float f = s2 * sv, f5 = f * s2;
+              const float4 q0 = pb[PKV * bi], q1 = pb[PKV * bi + 1], q2 = pb[PKV * bi + 2];
+              const float2 q3 = *(const float2 *)(pb + PKV * bi + 3);
+              const float Gb = q0.x, Mb0 = q0.y, Mb1 = q0.z, Mb2 = q0.w;
+              const float E0 = q1.x, E1 = q1.y, E2 = q1.z, H0 = q1.w, H1 = q2.x, H2 = q2.y;
+              const float rge = fmaf(rx, gE0, ejk);
+              const float w1 = fmaf(rx, -gB2, w1k);
+              const float w2 = fmaf(rx, gB1, w2j);
+              const float rc1 = fmaf(Gb, rge, fmaf(Mb2, w2, fmaf(Mb1, w1, Mb0 * w0)));
+              const float er = fmaf(rz, E2, fmaf(ry, E1, rx * E0));
+              const float v1 = fmaf(rx, -Ma2, v1k);
+              const float v2 = fmaf(rx, Ma1, v2j);
+              const float rc = fmaf(H2, v2, fmaf(H1, v1, fmaf(H0, v0, fmaf(-Ga, er, rc1))));
+              const float wp = (f5 * tt) * rc1;
+              ap0 = fmaf(wp, rx, ap0);
+              ap1 = fmaf(wp, ry, ap1);
+              ap2 = fmaf(wp, rz, ap2);
+              const float fr = f5 * rc;
+              aw0 = fmaf(fr, rx, aw0);
+              aw1 = fmaf(fr, ry, aw1);
+              aw2 = fmaf(fr, rz, aw2);
+              sp = fmaf(fr, tt, sp);  // the (p.R) p part: p is the same for every evaluation
+              SfG = fmaf(f, Gb, SfG);
+              SfM0 = fmaf(f, Mb0, SfM0);
+              SfM1 = fmaf(f, Mb1, SfM1);
+              SfM2 = fmaf(f, Mb2, SfM2);
+              SfE0 = fmaf(f, E0, SfE0);
+              SfE1 = fmaf(f, E1, SfE1);
+              SfE2 = fmaf(f, E2, SfE2);
+              SfH0 = fmaf(f, H0, SfH0);
+              SfH1 = fmaf(f, H1, SfH1);
+              SfH2 = fmaf(f, H2, SfH2);
+              Sfe = fmaf(f, q2.z, Sfe);
+              Sfh0 = fmaf(f, q2.w, Sfh0);
+              Sfh1 = fmaf(f, q3.x, Sfh1);
+              Sfh2 = fmaf(f, q3.y, Sfh2);
+            }
+          }
+        }
+        // this source pair's contributions, combined in FP32
+        const float xa = (float)tx, ya = (float)ty, za = (float)tz;
+        const float px = (float)consts[0];
+        float part[NF];
+        // gx = gE_a SfG + gB_a x SfM - Gamma_a SfE + M_a x SfH - 3 (aw + sp p)
+        part[0] = fmaf(-3.f, fmaf(sp, px, aw0), gE0 * SfG + (gB1 * SfM2 - gB2 * SfM1) +
+                                                    (Ma1 * SfH2 - Ma2 * SfH1) - Ga * SfE0);
+        part[1] = fmaf(-3.f, fmaf(sp, py, aw1), gE1 * SfG + (gB2 * SfM0 - gB0 * SfM2) +
+                                                    (Ma2 * SfH0 - Ma0 * SfH2) - Ga * SfE1);
+        part[2] = fmaf(-3.f, fmaf(sp, pz, aw2), gE2 * SfG + (gB0 * SfM1 - gB1 * SfM0) +
+                                                    (Ma0 * SfH1 - Ma1 * SfH0) - Ga * SfE2);
+        // sum f R.gE_b and sum f R x gB_b (subtracted from the moment adjoints)
+        part[3] = fmaf(za, SfE2, fmaf(ya, SfE1, xa * SfE0)) - Sfe;
+        part[4] = (ya * SfH2 - za * SfH1) - Sfh0;
+        part[5] = (za * SfH0 - xa * SfH2) - Sfh1;
+        part[6] = (xa * SfH1 - ya * SfH0) - Sfh2;
+        part[7] = ap0;
+        part[8] = ap1;
+        part[9] = ap2;
+#pragma unroll
+        for (int q = 0; q < NF; ++q) s_acc[q * BT + tid] += (double)part[q];
+      }
+      __syncthreads();  // the packed data and buffer bb are rewritten later
+    }
+  }
+  __syncthreads();  // s_ct
+  // moment adjoints (source role), the box from the node-position gradients, d/dp_avg
+  double gbx[6] = {0, 0, 0, 0, 0, 0};
+  double gpv[6] = {0, 0, 0, 0, 0, 0};
+  if (act) {
+    double v[NF];
+#pragma unroll
+    for (int q = 0; q < NF; ++q) v[q] = s_acc[q * BT + tid];
+    double *gm = gmom + (int64_t)t * 4 * NN;
+    gm[a] -= v[3];
+    gm[NN + a] -= v[4];
+    gm[2 * NN + a] -= v[5];
+    gm[3 * NN + a] -= v[6];
+    const int idx[3] = {a % M, (a / M) % M, a / (M * M)};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      gbx[d] += (1.0 - s_ct[idx[d]]) * v[d];
+      gbx[3 + d] += s_ct[idx[d]] * v[d];
+      gpv[d] += -3.0 * v[7 + d];
+    }
+  }
+  block_sum<6>(gbx, s_red);
+  if (tid < 6) gbox[6 * (int64_t)t + tid] += gbx[tid];
+  block_sum<6>(gpv, s_red);
+  if (tid < 3) gp_part[3 * (int64_t)t + tid] = gpv[tid];
+}
+
 // ---------------------------------------------------------------- P2P^T (per target leaf)
 // Per target particle p over the particles j of every source leaf in the union list:
 //   (t <- s), flag 1: K1 = K(R; u_j), c1 = gamma_j a_E,p + a_B,p x u_j:
@@ -1317,12 +1569,23 @@ int run_backward_t(Ctx *ctx, const double *d_ge, const double *d_gb, double *d_g
     FMM_TRY(ctx->ensure("bwd_rec32", (int64_t)S2::RECF * nc, &rec32));
     adj_rec32_kernel<NDEG><<<592, 256, 0, st>>>(nc, ctx->get<float>("mom32"), gloc, rec32);
     FMM_TRY(ctx->check_launch("adj_rec32_kernel"));
-    auto k = mask ? m2l_bwd_x2_kernel<NDEG, true> : m2l_bwd_x2_kernel<NDEG, false>;
-    FMM_TRY(opt_in_smem(ctx, k, S2::SMEM));
-    k<<<(unsigned)nc, S2::BT, S2::SMEM, st>>>(ctx->get<int>("m2lu_ptr"), ctx->get<int>("m2lu_src"),
-                                              ctx->get<uint8_t>("m2lu_flag"), nodes, bbox, ct, rec32,
-                                              ctx->get<double>("consts"), gmom, gbox, gpp, ctx->d_status);
-    FMM_TRY(ctx->check_launch("m2l_bwd_x2_kernel"));
+    // n = 8 keeps the packed kernel: one node per thread would need 736 threads per CTA
+    if (mask || NDEG >= 8) {
+      auto k = mask ? m2l_bwd_x2_kernel<NDEG, true> : m2l_bwd_x2_kernel<NDEG, false>;
+      FMM_TRY(opt_in_smem(ctx, k, S2::SMEM));
+      k<<<(unsigned)nc, S2::BT, S2::SMEM, st>>>(ctx->get<int>("m2lu_ptr"), ctx->get<int>("m2lu_src"),
+                                                ctx->get<uint8_t>("m2lu_flag"), nodes, bbox, ct, rec32,
+                                                ctx->get<double>("consts"), gmom, gbox, gpp, ctx->d_status);
+      FMM_TRY(ctx->check_launch("m2l_bwd_x2_kernel"));
+    } else if constexpr (NDEG < 8) {
+      using SF = MBShape1F<NDEG>;
+      auto k = m2l_bwd_x1f_kernel<NDEG>;
+      FMM_TRY(opt_in_smem(ctx, k, SF::SMEM));
+      k<<<(unsigned)nc, SF::BT, SF::SMEM, st>>>(ctx->get<int>("m2lu_ptr"), ctx->get<int>("m2lu_src"),
+                                                ctx->get<uint8_t>("m2lu_flag"), nodes, bbox, ct, rec32,
+                                                ctx->get<double>("consts"), gmom, gbox, gpp, ctx->d_status);
+      FMM_TRY(ctx->check_launch("m2l_bwd_x1f_kernel"));
+    }
   } else {
     auto k = mask ? m2l_bwd_kernel<NDEG, true> : m2l_bwd_kernel<NDEG, false>;
     const int sm = 2 * (10 * NN + NS) * 8;

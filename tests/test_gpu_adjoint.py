@@ -119,11 +119,14 @@ def test_mixed_forward_adjoint_matches_fp64(gpu_ctx):
 
 @pytest.mark.parametrize("kind,N,n,N0,eta", [("gauss", 30000, 4, 125, 0.5), ("gauss", 30000, 4, 32, 0.5),
                                               ("uniform", 20000, 3, 100, 0.5), ("beamlets", 20000, 2, 200, 0.5),
-                                              ("gauss", 20000, 4, 64, 0.7), ("duplicates", 20000, 4, 64, 0.5)])
+                                              ("gauss", 20000, 4, 64, 0.7), ("duplicates", 20000, 4, 64, 0.5),
+                                              ("gauss", 20000, 1, 32, 0.5), ("gauss", 30000, 6, 400, 0.5),
+                                              ("uniform", 30000, 7, 600, 0.5), ("gauss", 30000, 8, 800, 0.5)])
 def test_mixed_adjoint_kernels_match_fp64(gpu_ctx, kind, N, n, N0, eta):
-    """The mixed form's adjoint runs M2L^T and P2P^T in packed FP32 (hi/lo
-    coordinates in the near field); it stays within 1e-4 of the FP64 adjoint for
-    every lane-group width (leaf sizes 32..256) and for eta > 1/2 (masked nodes)."""
+    """The mixed form's adjoint runs M2L^T and P2P^T in FP32 (hi/lo coordinates in
+    the near field); it stays within 1e-4 of the FP64 adjoint for every lane-group
+    width (leaf sizes 32..256), for eta > 1/2 (masked nodes, packed unfactored
+    M2L^T), for n = 1..7 (scalar factored M2L^T) and n = 8 (packed unfactored)."""
     import fmmb200
     from fmmb200 import beams
 
