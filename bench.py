@@ -25,6 +25,10 @@ bit-identical to serial) on a bounded sample of the same workload.
 
 Multi-GPU (--gpus N under torchrun): the field evaluation is replicated, one
 independent beam per rank (weak scaling); the timing is the max over ranks.
+With --shard, one beam of --N particles is split over the ranks instead (strong
+scaling): each step all-gathers positions and momenta, every rank builds the tree
+and lists of the whole beam and evaluates its share of the leaves, and a
+reduce-scatter returns each rank the fields of its own particles.
 """
 from __future__ import annotations
 
@@ -74,6 +78,9 @@ def parse():
     ap.add_argument("--m2l-engine", choices=["auto", "cuda_cores", "tensor_cores"], default="auto",
                     help="mixed-form M2L engine (fmmb200_set_m2l_engine)")
     ap.add_argument("--bwd-steps", type=int, default=3, help="timed fwd+bwd steps (after 2 warm-up steps)")
+    ap.add_argument("--shard", action="store_true",
+                    help="one beam of --N particles split over the ranks (strong scaling, fmmb200.sharded) "
+                         "instead of one independent beam per rank")
     return ap.parse_args()
 
 
@@ -467,6 +474,67 @@ def run_ours(args, world, rank, local):
     ctx.close()
 
 
+def run_sharded(args, world, rank, local):
+    """One beam of args.N particles over the ranks: mixed form, device-resident, the
+    exchange (all-gather in, reduce-scatter out) inside the timed region."""
+    import torch
+
+    import fmmb200
+    from fmmb200 import sharded
+
+    dev = torch.device("cuda", local)
+    N = args.N
+    pos_h, mom_h = generate(args, N, args.seed)
+    lo, hi = N * rank // world, N * (rank + 1) // world
+    pos = torch.from_numpy(pos_h[lo:hi]).to(dev)
+    mom = torch.from_numpy(mom_h[lo:hi]).to(dev)
+    ctx = fmmb200.Context(local)
+    ctx.set_timing(True)
+    alg = fmmb200.FMMB200(n=args.n, N0=args.N0, eta=args.eta, precision="mixed")
+
+    def step():
+        return sharded.sharded_fields(pos, mom, alg, ctx=ctx)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    except Exception:
+        pass
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(uuid) as clk:
+        ev0.record()
+        for _ in range(args.steps):
+            E, B = step()
+        ev1.record()
+        ev1.synchronize()
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    ms = max_over_ranks(world, ev0.elapsed_time(ev1) / args.steps)
+    st = ctx.stats()
+    if rank == 0:
+        cfg = workload(args)
+        cfg["workload"] = cfg["workload"].replace("value = mixed form, fp64 = plain path",
+                                                  f"one beam split over {world} rank(s), mixed form")
+        cfg["parallelism"] = f"shard{world}"
+        print(json.dumps({
+            "metric": METRIC, "value": N / (ms * 1e-3), "unit": "particles/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic: one seeded Gaussian bunch split over the ranks", "config": cfg,
+            "shard": {"particles_per_rank": hi - lo, "allgather_bytes_per_rank": 48 * N,
+                      "reduce_scatter_bytes_per_rank": 48 * N, "ms_m2l_rank0": st["ms_m2l"],
+                      "ms_p2p_rank0": st["ms_p2p"], "ms_tree_rank0": st["ms_tree"]},
+            "gpu_launches": int(st["kernel_launches"]) * args.steps,
+            "clocks": clk.summary(),
+        }), flush=True)
+    ctx.close()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -475,7 +543,7 @@ def main():
         return
     world, rank, local = dist_setup(args)
     try:
-        run_ours(args, world, rank, local)
+        (run_sharded if args.shard else run_ours)(args, world, rank, local)
     finally:
         if world > 1:
             import torch.distributed as dist

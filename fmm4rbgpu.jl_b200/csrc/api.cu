@@ -45,6 +45,35 @@ __global__ void finite_check_kernel(const double *__restrict__ a, int64_t n, int
   if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicExch(flag, 1);
 }
 
+// Sharded forward (fmmb200_set_shard): heap cluster c at level l covers the leaves
+// [(c + 1 - 2^l) 2^(ml - l), (c + 2 - 2^l) 2^(ml - l)); a shard keeps the M2L rows of
+// the clusters whose leaves meet its own [lo, hi).  cnt has nc + 1 entries (the last 0).
+__device__ __forceinline__ bool shard_owns(int64_t c, int ml, int64_t lo, int64_t hi) {
+  const int l = 63 - __clzll((long long)(c + 1));
+  const int64_t first = (c + 1 - (1ll << l)) << (ml - l), last = first + (1ll << (ml - l));
+  return first < hi && last > lo;
+}
+
+__global__ void shard_rows_kernel(int64_t nc, int ml, int64_t lo, int64_t hi, const int *__restrict__ ptr,
+                                  int *__restrict__ cnt) {
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c > nc) return;
+  cnt[c] = (c < nc && shard_owns(c, ml, lo, hi)) ? ptr[c + 1] - ptr[c] : 0;
+}
+
+__global__ void shard_copy_kernel(int64_t nc, int ml, int64_t lo, int64_t hi, const int *__restrict__ ptr,
+                                  const int *__restrict__ src, const int *__restrict__ ptr2, int *__restrict__ src2) {
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc || !shard_owns(c, ml, lo, hi)) return;
+  const int b = ptr[c], e = ptr[c + 1], o = ptr2[c];
+  for (int k = b; k < e; ++k) src2[o + k - b] = src[k];
+}
+
+__global__ void iota_kernel(int first, int n, int *__restrict__ ids) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) ids[i] = first + i;
+}
+
 __global__ void widen_kernel(const float *__restrict__ a, int64_t n, double *__restrict__ b) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     b[i] = (double)a[i];
@@ -97,12 +126,44 @@ int ensure_expansions(Ctx *ctx, int n, bool mixed) {
   return FMMB200_OK;
 }
 
+// A shard's own leaves (ids) and its compacted M2L target lists, which the M2L
+// launchers read until the keys are reset.
+int prepare_shard(Ctx *ctx, const int **ids, int64_t *n_own) {
+  const int64_t nl = ctx->nleaf, w = ctx->shard_world, r = ctx->shard_rank;
+  const int64_t lo = nl * r / w, hi = nl * (r + 1) / w, nc = ctx->nc;
+  int *d_ids, *cnt, *ptr2, *src2;
+  FMM_TRY(ctx->ensure("shard_leaves", hi > lo ? hi - lo : 1, &d_ids));
+  FMM_TRY(ctx->ensure("shard_cnt", nc + 1, &cnt));
+  FMM_TRY(ctx->ensure("m2l_ptr_sh", nc + 1, &ptr2));
+  FMM_TRY(ctx->ensure("m2l_src_sh", ctx->nm2l > 0 ? ctx->nm2l : 1, &src2));
+  if (hi > lo) {
+    iota_kernel<<<ceil_div(hi - lo, 256), 256, 0, ctx->stream>>>((int)(ctx->leaf0 + lo), (int)(hi - lo), d_ids);
+    FMM_TRY(ctx->check_launch("iota_kernel"));
+  }
+  const int *ptr = ctx->get<int>("m2l_ptr"), *src = ctx->get<int>("m2l_src");
+  shard_rows_kernel<<<ceil_div(nc + 1, 256), 256, 0, ctx->stream>>>(nc, ctx->ml, lo, hi, ptr, cnt);
+  FMM_TRY(ctx->check_launch("shard_rows_kernel"));
+  FMM_TRY(exclusive_scan_i32(ctx, cnt, ptr2, nc + 1, nullptr));
+  shard_copy_kernel<<<ceil_div(nc, 256), 256, 0, ctx->stream>>>(nc, ctx->ml, lo, hi, ptr, src, ptr2, src2);
+  FMM_TRY(ctx->check_launch("shard_copy_kernel"));
+  ctx->m2l_ptr_key = "m2l_ptr_sh";
+  ctx->m2l_src_key = "m2l_src_sh";
+  *ids = d_ids;
+  *n_own = hi - lo;
+  return FMMB200_OK;
+}
+
 // The device forward.  d_pos/d_mom: AoS device arrays; d_E/d_B: AoS outputs.
 int run_forward(Ctx *ctx, int64_t N, const double *d_pos, const double *d_mom, double charge, double lambda, int n,
                 int64_t N0, double eta, int precision, const double *pavg_host, bool save, double *d_E,
                 double *d_B) {
   const bool mixed = precision == FMMB200_PRECISION_MIXED;
   const int64_t launches0 = ctx->launches;
+  const bool sharded = ctx->shard_world > 1;
+  if (sharded && save)
+    return ctx->fail(FMMB200_ERR_INVALID_ARGUMENT, "save_for_backward needs an unsharded forward (world 1)");
+  ctx->m2l_ptr_key = "m2l_ptr";
+  ctx->m2l_src_key = "m2l_src";
   double *consts;
   int *flag;
   FMM_TRY(ctx->ensure("consts", 8, &consts));
@@ -138,15 +199,26 @@ int run_forward(Ctx *ctx, int64_t N, const double *d_pos, const double *d_mom, d
   // dual-tree traversal (:112-116, 123-125)
   FMM_TRY(build_lists(ctx, eta, consts));
   mark(ctx, kEvLists);
+  // a shard: its own leaves and the M2L rows of the clusters above them
+  const int *own = nullptr;
+  int64_t n_own = ctx->nleaf;
+  if (sharded) FMM_TRY(prepare_shard(ctx, &own, &n_own));
   // interactions (:118-128)
-  FMM_TRY(launch_m2l(ctx, n, mixed, false));
+  const int m2l_st = launch_m2l(ctx, n, mixed, false);
+  ctx->m2l_ptr_key = "m2l_ptr";
+  ctx->m2l_src_key = "m2l_src";
+  FMM_TRY(m2l_st);
   mark(ctx, kEvM2L);
-  FMM_TRY(launch_p2p(ctx, mixed, nullptr, ctx->nleaf, false));
+  FMM_TRY(launch_p2p(ctx, mixed, own, n_own, false));
   mark(ctx, kEvP2P);
   // downward pass, amp and write-back (:130-147)
   for (int l = 1; l <= ctx->ml; ++l) FMM_TRY(launch_l2l(ctx, n, mixed, l));
   const double amp = kRe * charge / lambda;
-  FMM_TRY(launch_l2p(ctx, n, mixed, nullptr, ctx->nleaf, 1, amp, d_E, d_B));
+  if (sharded) {  // the other shards' particles read 0
+    FMM_CUDA_TRY(ctx, cudaMemsetAsync(d_E, 0, sizeof(double) * 3 * N, ctx->stream));
+    FMM_CUDA_TRY(ctx, cudaMemsetAsync(d_B, 0, sizeof(double) * 3 * N, ctx->stream));
+  }
+  FMM_TRY(launch_l2p(ctx, n, mixed, own, n_own, 1, amp, d_E, d_B));
   mark(ctx, kEvDown);
   FMM_TRY(ctx->check_device_status("forward"));
   int *h;
@@ -437,6 +509,15 @@ int fmmb200_set_m2l_engine(fmmb200_ctx *ctx, int engine) {
 int fmmb200_set_tree_reuse(fmmb200_ctx *ctx, int enable) {
   if (!ctx) return FMMB200_ERR_INVALID_ARGUMENT;
   ctx->tree_reuse = enable != 0;
+  return FMMB200_OK;
+}
+
+int fmmb200_set_shard(fmmb200_ctx *ctx, int rank, int world) {
+  if (!ctx) return FMMB200_ERR_INVALID_ARGUMENT;
+  if (world < 1 || rank < 0 || rank >= world)
+    return ctx->fail(FMMB200_ERR_INVALID_ARGUMENT, "shard: need 0 <= rank < world");
+  ctx->shard_rank = rank;
+  ctx->shard_world = world;
   return FMMB200_OK;
 }
 

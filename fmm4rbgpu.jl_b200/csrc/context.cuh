@@ -47,6 +47,11 @@ struct fmmb200_ctx {
   int list_bits = 1;  // pair keys are (target << list_bits) | source
   int m2l_engine = 0;  // FMMB200_M2L_*: mixed-form M2L engine
   bool tree_reuse = false;  // forward: refit the previous tree when it is still exact
+  // forward: fields of the leaves [rank nleaf / world, (rank + 1) nleaf / world) only
+  int shard_rank = 0, shard_world = 1;
+  // the M2L target lists the M2L launchers read (a shard's compacted copy, or all)
+  const char *m2l_ptr_key = "m2l_ptr";
+  const char *m2l_src_key = "m2l_src";
   fmmb200_stats stats{};
 
   // pairwise-summation plan for p_avg (depends on N only)

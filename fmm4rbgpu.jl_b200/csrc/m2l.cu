@@ -732,7 +732,7 @@ int launch_m2l_fp64(Ctx *ctx, bool accumulate) {
   FMM_TRY(opt_in_smem(ctx, kern, smem));
   if (ctx->nc > 0)
     kern<<<(unsigned)ctx->nc, S::BT, smem, ctx->stream>>>(
-        ctx->get<int>("m2l_ptr"), ctx->get<int>("m2l_src"), ctx->get<double>("nodes"), ctx->get<double>("bbox"),
+        ctx->get<int>(ctx->m2l_ptr_key), ctx->get<int>(ctx->m2l_src_key), ctx->get<double>("nodes"), ctx->get<double>("bbox"),
         ctx->get<double>("mom64"), ctx->get<double>("loc64"), ctx->get<double>("consts"), accumulate ? 1 : 0,
         ctx->d_status);
   return ctx->check_launch("m2l_kernel");
@@ -745,7 +745,7 @@ int launch_m2l_tc(Ctx *ctx, bool accumulate) {
   FMM_TRY(opt_in_smem(ctx, kern, S::SMEM));
   if (ctx->nc > 0)
     kern<<<(unsigned)ctx->nc, kTcThreads, S::SMEM, ctx->stream>>>(
-        ctx->get<int>("m2l_ptr"), ctx->get<int>("m2l_src"), ctx->get<double>("nodes"), ctx->get<double>("bbox"),
+        ctx->get<int>(ctx->m2l_ptr_key), ctx->get<int>(ctx->m2l_src_key), ctx->get<double>("nodes"), ctx->get<double>("bbox"),
         ctx->get<float>("mom32"), ctx->get<float>("loc32"), ctx->get<double>("consts"), accumulate ? 1 : 0,
         ctx->d_status);
   return ctx->check_launch("m2l_tc_kernel");
@@ -762,7 +762,7 @@ int launch_m2l_mixed(Ctx *ctx, bool accumulate) {
   FMM_TRY(opt_in_smem(ctx, kern, S::SMEM));
   if (ctx->nc > 0)
     kern<<<(unsigned)ctx->nc, S::BT, S::SMEM, ctx->stream>>>(
-        ctx->get<int>("m2l_ptr"), ctx->get<int>("m2l_src"), ctx->get<double>("nodes"), ctx->get<double>("bbox"),
+        ctx->get<int>(ctx->m2l_ptr_key), ctx->get<int>(ctx->m2l_src_key), ctx->get<double>("nodes"), ctx->get<double>("bbox"),
         ctx->get<float>("mom32"), ctx->get<float>("loc32"), ctx->get<double>("consts"), accumulate ? 1 : 0,
         ctx->d_status);
   return ctx->check_launch("m2l_x2_kernel");

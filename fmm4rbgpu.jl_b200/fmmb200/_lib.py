@@ -107,6 +107,7 @@ SIGNATURES = {
     "fmmb200_measure_fma_peak": (ctypes.c_int, [c_vp, p_f64, p_f64, p_f64]),
     "fmmb200_set_m2l_engine": (ctypes.c_int, [c_vp, ctypes.c_int]),
     "fmmb200_set_tree_reuse": (ctypes.c_int, [c_vp, ctypes.c_int]),
+    "fmmb200_set_shard": (ctypes.c_int, [c_vp, ctypes.c_int, ctypes.c_int]),
     "fmmb200_direct_noalloc": (ctypes.c_int, [c_i64, c_vp, c_vp, c_f64, c_f64, c_i64, c_vp, c_vp, c_vp, c_vp]),
 }
 

@@ -157,6 +157,12 @@ class Context:
         way (checked exactly on the device); see fmmb200_set_tree_reuse."""
         self._check(self._lib.fmmb200_set_tree_reuse(self._h, int(bool(enable))))
 
+    def set_shard(self, rank: int, world: int):
+        """Later forwards compute only the fields of the particles in this shard's
+        leaves (rank of world) and write 0 for every other particle; the sum over the
+        shards is the unsharded result bit for bit.  See fmmb200_set_shard."""
+        self._check(self._lib.fmmb200_set_shard(self._h, int(rank), int(world)))
+
     def debug_fail_alloc(self, k: int):
         self._check(self._lib.fmmb200_debug_fail_alloc(self._h, int(k)))
 

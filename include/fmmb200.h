@@ -94,6 +94,16 @@ int fmmb200_set_m2l_engine(fmmb200_ctx *ctx, int engine);
  * and the radix sorts and partitions are skipped; otherwise the tree is rebuilt.  For
  * time-stepping loops whose particles move little per step.  Off by default. */
 int fmmb200_set_tree_reuse(fmmb200_ctx *ctx, int enable);
+/* One beam over several GPUs (no counterpart in the reference, whose FMMGPU runs on one
+ * GPU).  With world > 1, each forward builds the whole tree, the pair lists and all
+ * moments from the whole beam, then runs M2L, P2P, L2L and L2P only for the clusters over
+ * the leaves [rank nleaf / world, (rank + 1) nleaf / world) (heap order) and writes the
+ * fields of the particles in those leaves; every other particle's field is set to 0.
+ * The sum over rank = 0 .. world-1 is bit-identical to the unsharded forward, so the
+ * caller combines the ranks with one sum-reduction (reduce-scatter or all-reduce).  The
+ * adjoint needs an unsharded forward: save_for_backward with world > 1 is rejected.
+ * 0 <= rank < world; world = 1 (the default) computes every field. */
+int fmmb200_set_shard(fmmb200_ctx *ctx, int rank, int world);
 /* Fault injection for tests: the k-th next device allocation fails (k >= 1; 0 disables). */
 int fmmb200_debug_fail_alloc(fmmb200_ctx *ctx, int64_t k);
 

@@ -60,6 +60,7 @@ def test_null_and_bad_arguments_return_status_without_gpu():
     assert lib.fmmb200_set_timing(None, 1) == fmmb200.ERR_INVALID_ARGUMENT
     assert lib.fmmb200_set_m2l_engine(None, 0) == fmmb200.ERR_INVALID_ARGUMENT
     assert lib.fmmb200_set_tree_reuse(None, 1) == fmmb200.ERR_INVALID_ARGUMENT
+    assert lib.fmmb200_set_shard(None, 0, 1) == fmmb200.ERR_INVALID_ARGUMENT
 
 
 def test_create_without_a_device_fails_cleanly():
