@@ -154,9 +154,11 @@ int prepare_shard(Ctx *ctx, const int **ids, int64_t *n_own) {
 }
 
 // The device forward.  d_pos/d_mom: AoS device arrays; d_E/d_B: AoS outputs.
+// mom_ready (optional): an event after which d_mom holds the momenta; the work before
+// it (finite check of the positions, the radix sorts of the tree build) reads only d_pos.
 int run_forward(Ctx *ctx, int64_t N, const double *d_pos, const double *d_mom, double charge, double lambda, int n,
                 int64_t N0, double eta, int precision, const double *pavg_host, bool save, double *d_E,
-                double *d_B) {
+                double *d_B, cudaEvent_t mom_ready = nullptr) {
   const bool mixed = precision == FMMB200_PRECISION_MIXED;
   const int64_t launches0 = ctx->launches;
   const bool sharded = ctx->shard_world > 1;
@@ -170,19 +172,30 @@ int run_forward(Ctx *ctx, int64_t N, const double *d_pos, const double *d_mom, d
   FMM_TRY(ctx->ensure("finite_flag", 1, &flag));
   FMM_CUDA_TRY(ctx, cudaMemsetAsync(flag, 0, sizeof(int), ctx->stream));
   finite_check_kernel<<<592, 256, 0, ctx->stream>>>(d_pos, 3 * N, flag);
-  finite_check_kernel<<<592, 256, 0, ctx->stream>>>(d_mom, 3 * N, flag);
-  FMM_TRY(ctx->check_launch("finite_check_kernel", 2));
-  if (pavg_host) {
-    FMM_CUDA_TRY(ctx, cudaMemcpyAsync(consts, pavg_host, 3 * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-    stretch_kernel<<<1, 1, 0, ctx->stream>>>(consts);
-    FMM_TRY(ctx->check_launch("stretch_kernel"));
-  } else {
-    FMM_TRY(compute_pavg_stretch(ctx, d_mom, N, consts));
-  }
+  FMM_TRY(ctx->check_launch("finite_check_kernel"));
+  // everything that reads the momenta: their finite check and p_avg / stretch
+  bool mom_done = false;
+  auto momentum_steps = [&]() -> int {
+    if (mom_done) return FMMB200_OK;
+    mom_done = true;
+    if (mom_ready) FMM_CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->stream, mom_ready, 0));
+    finite_check_kernel<<<592, 256, 0, ctx->stream>>>(d_mom, 3 * N, flag);
+    FMM_TRY(ctx->check_launch("finite_check_kernel"));
+    if (pavg_host) {
+      FMM_CUDA_TRY(ctx, cudaMemcpyAsync(consts, pavg_host, 3 * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+      stretch_kernel<<<1, 1, 0, ctx->stream>>>(consts);
+      return ctx->check_launch("stretch_kernel");
+    }
+    return compute_pavg_stretch(ctx, d_mom, N, consts);
+  };
   ctx->pavg_from_momenta = pavg_host == nullptr;
   bool reused = false;
-  if (ctx->tree_reuse) FMM_TRY(refit_tree(ctx, d_pos, N, N0, consts, &reused));
-  if (!reused) FMM_TRY(build_tree(ctx, d_pos, N, N0, consts));
+  if (ctx->tree_reuse) {  // the refit checks the splits with the stretch
+    FMM_TRY(momentum_steps());
+    FMM_TRY(refit_tree(ctx, d_pos, N, N0, consts, &reused));
+  }
+  if (!reused) FMM_TRY(build_tree(ctx, d_pos, N, N0, consts, momentum_steps));
+  FMM_TRY(momentum_steps());
   FMM_TRY(gather_particles(ctx, d_pos, d_mom, mixed));
   FMM_TRY(compute_nodes(ctx, n));
   ctx->n = n;
@@ -456,15 +469,22 @@ int fmmb200_create(fmmb200_ctx **out, int device) {
   if (device < 0 || device >= ndev) return FMMB200_ERR_INVALID_ARGUMENT;
   Ctx *ctx = new Ctx();
   ctx->device = device;
-  Guard g(ctx);
-  if (cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaMalloc(&ctx->d_status, sizeof(int)) != cudaSuccess ||
-      cudaMemset(ctx->d_status, 0, sizeof(int)) != cudaSuccess) {
-    cudaGetLastError();
-    delete ctx;
+  bool ok;
+  {
+    Guard g(ctx);
+    ok = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) == cudaSuccess &&
+         cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking) == cudaSuccess &&
+         cudaEventCreateWithFlags(&ctx->ev_copy[0], cudaEventDisableTiming) == cudaSuccess &&
+         cudaEventCreateWithFlags(&ctx->ev_copy[1], cudaEventDisableTiming) == cudaSuccess &&
+         cudaMalloc(&ctx->d_status, sizeof(int)) == cudaSuccess &&
+         cudaMemset(ctx->d_status, 0, sizeof(int)) == cudaSuccess;
+    if (!ok) cudaGetLastError();
+    ctx->stream = ctx->own_stream;
+  }
+  if (!ok) {  // releases whatever was created
+    fmmb200_destroy(ctx);
     return FMMB200_ERR_CUDA;
   }
-  ctx->stream = ctx->own_stream;
   *out = ctx;
   return FMMB200_OK;
 }
@@ -480,6 +500,10 @@ int fmmb200_destroy(fmmb200_ctx *ctx) {
     if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
     if (ctx->ev_ready)
       for (auto &e : ctx->ev) cudaEventDestroy(e);
+    if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
+    for (auto &e : ctx->ev_copy)
+      if (e) cudaEventDestroy(e);
+    if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
   }
   delete ctx;
@@ -561,10 +585,22 @@ int fmmb200_forward(fmmb200_ctx *ctx, int64_t npar, const double *pos, const dou
   FMM_TRY(ctx->ensure("out_e", 3 * npar, &de));
   FMM_TRY(ctx->ensure("out_b", 3 * npar, &db));
   mark(ctx, kEvStart);
+  // positions on the stream; momenta on the copy stream, overlapping the position-only
+  // start of the tree build (finite check, radix sorts)
+  FMM_CUDA_TRY(ctx, cudaEventRecord(ctx->ev_copy[0], ctx->stream));
   FMM_CUDA_TRY(ctx, cudaMemcpyAsync(dp, pos, sizeof(double) * 3 * npar, cudaMemcpyHostToDevice, ctx->stream));
-  FMM_CUDA_TRY(ctx, cudaMemcpyAsync(dm, mom, sizeof(double) * 3 * npar, cudaMemcpyHostToDevice, ctx->stream));
+  FMM_CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->copy_stream, ctx->ev_copy[0], 0));
+  FMM_CUDA_TRY(ctx, cudaMemcpyAsync(dm, mom, sizeof(double) * 3 * npar, cudaMemcpyHostToDevice, ctx->copy_stream));
+  FMM_CUDA_TRY(ctx, cudaEventRecord(ctx->ev_copy[1], ctx->copy_stream));
   mark(ctx, kEvH2D);
-  FMM_TRY(run_forward(ctx, npar, dp, dm, charge, lambda, n, N0, eta, precision, pavg, save_for_backward != 0, de, db));
+  const int fs = run_forward(ctx, npar, dp, dm, charge, lambda, n, N0, eta, precision, pavg, save_for_backward != 0,
+                             de, db, ctx->ev_copy[1]);
+  if (fs != FMMB200_OK) {  // the caller's buffers must outlive the copies in flight
+    cudaStreamSynchronize(ctx->copy_stream);
+    cudaStreamSynchronize(ctx->stream);
+    cudaGetLastError();
+    return fs;
+  }
   FMM_CUDA_TRY(ctx, cudaMemcpyAsync(efields, de, sizeof(double) * 3 * npar, cudaMemcpyDeviceToHost, ctx->stream));
   FMM_CUDA_TRY(ctx, cudaMemcpyAsync(bfields, db, sizeof(double) * 3 * npar, cudaMemcpyDeviceToHost, ctx->stream));
   mark(ctx, kEvD2H);

@@ -12,6 +12,10 @@ struct fmmb200_ctx {
   int device = 0;
   cudaStream_t own_stream = nullptr;
   cudaStream_t stream = nullptr;
+  // the host-pointer forward copies the momenta here while the stream starts the tree
+  // build on the positions; ev_copy[0]: inputs free to overwrite, [1]: momenta copied
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t ev_copy[2] = {};
   std::string err;
   int64_t fail_alloc_countdown = 0;  // >0: the countdown-th next allocation fails
   bool timing = false;

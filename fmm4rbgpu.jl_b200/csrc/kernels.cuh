@@ -1,6 +1,8 @@
 // kernels.cuh -- host-side launchers shared between the translation units.
 #pragma once
 
+#include <functional>
+
 #include "context.cuh"
 
 namespace fmmb200 {
@@ -30,7 +32,10 @@ int exclusive_scan_i32(Ctx *ctx, const int *in, int *out, int64_t n, int64_t *to
 int compute_pavg_stretch(Ctx *ctx, const double *d_mom_aos, int64_t N, double *d_consts);
 // Build the cluster tree of N particles (AoS positions on device) with the
 // stretch in d_consts[3..5]; fills ctx tree buffers and ctx->{N,N0,ml,nc,...}.
-int build_tree(Ctx *ctx, const double *d_pos_aos, int64_t N, int64_t N0, const double *d_consts);
+// after_sorts, if given, is called once the three coordinate orders are sorted and
+// before anything reads d_consts (the radix sorts need the positions only).
+int build_tree(Ctx *ctx, const double *d_pos_aos, int64_t N, int64_t N0, const double *d_consts,
+               const std::function<int()> &after_sorts = {});
 // Refit the existing tree (same N, N0) to new positions: boxes and extremal
 // particles bottom-up, and *same = true when every node would split as before, in
 // which case the tree equals what build_tree would give.  Otherwise the refitted

@@ -709,7 +709,8 @@ int compute_pavg_stretch(Ctx *ctx, const double *d_mom, int64_t N, double *d_con
   return ctx->check_launch("compute_pavg_stretch", 2);
 }
 
-int build_tree(Ctx *ctx, const double *d_pos, int64_t N64, int64_t N0, const double *d_consts) {
+int build_tree(Ctx *ctx, const double *d_pos, int64_t N64, int64_t N0, const double *d_consts,
+               const std::function<int()> &after_sorts) {
   if (N64 > 0x7FFFFFFF) return ctx->fail(FMMB200_ERR_INVALID_ARGUMENT, "npar must be < 2^31");
   const int N = (int)N64;
   // tree shape (treeinfo.jl:6-26) with the reference's floating-point formula
@@ -763,6 +764,7 @@ int build_tree(Ctx *ctx, const double *d_pos, int64_t N64, int64_t N0, const dou
     FMM_CUDA_TRY(ctx, cudaMemcpyAsync(lists + (int64_t)a * N, alt ? vB : vA, sizeof(uint32_t) * N,
                                       cudaMemcpyDeviceToDevice, ctx->stream));
   }
+  if (after_sorts) FMM_TRY(after_sorts());
   // 2. levels: globally down to L0, the first level whose nodes fit one CTA (and at
   // most 10 levels above the leaves), then each level-L0 subtree in shared memory
   int L0 = 0;
