@@ -987,6 +987,75 @@ __global__ void __launch_bounds__(MBShape1F<NDEG>::BT, MBShape1F<NDEG>::MINB)
             ryv[b] = (float)(ty - s_sn[M + b]);
           }
         }
+        float part[NF];
+        if (!factored_ok<M>(SN, tb, cx, cy, cz)) {
+          // boxes that nearly touch: the unfactored sums of m2l_bwd_x2_kernel
+          //   c = Gamma_b gE_a + gB_a x M_b - Gamma_a gE_b + M_a x gB_b,  c1 its first two terms
+          float ax0 = 0.f, ax1 = 0.f, ax2 = 0.f, aG = 0.f, aM0 = 0.f, aM1 = 0.f, aM2 = 0.f;
+          float aw0 = 0.f, aw1 = 0.f, aw2 = 0.f, sp = 0.f, ap0 = 0.f, ap1 = 0.f, ap2 = 0.f;
+#pragma unroll 1
+          for (int bk = 0; bk < M; ++bk) {
+            const float rz = (float)(tz - s_sn[2 * M + bk]);
+            const float prz = pz * rz;
+            const float rzz = fmaf(rz, rz, eps);
+#pragma unroll
+            for (int bj = 0; bj < M; ++bj) {
+              const float ry = ryv[bj];
+              const float P = fmaf(py, ry, prz);
+              const float A = fmaf(ry, ry, rzz);
+              const float4 *pb = pk + PKV * M * (bj + M * bk);
+#pragma unroll
+              for (int bi = 0; bi < M; ++bi) {
+                const float rx = rxv[bi];
+                const float tt = P + prx[bi];
+                const float d = fmaf(tt, tt, A + rx2[bi]);
+                const float sv = rsqrt_approx_f32(d);
+                const float s2 = sv * sv;
+                const float f = s2 * sv, f5 = f * s2;
+                const float4 q0 = pb[PKV * bi], q1 = pb[PKV * bi + 1];
+                const float2 q2 = *(const float2 *)(pb + PKV * bi + 2);
+                const float Gb = q0.x, Mb0 = q0.y, Mb1 = q0.z, Mb2 = q0.w;
+                const float E0 = q1.x, E1 = q1.y, E2 = q1.z, H0 = q1.w, H1 = q2.x, H2 = q2.y;
+                float c0 = fmaf(Gb, gE0, gB1 * Mb2 - gB2 * Mb1);
+                float c1 = fmaf(Gb, gE1, gB2 * Mb0 - gB0 * Mb2);
+                float c2 = fmaf(Gb, gE2, gB0 * Mb1 - gB1 * Mb0);
+                const float rc1 = fmaf(rz, c2, fmaf(ry, c1, rx * c0));
+                const float wp = (f5 * tt) * rc1;
+                ap0 = fmaf(wp, rx, ap0);
+                ap1 = fmaf(wp, ry, ap1);
+                ap2 = fmaf(wp, rz, ap2);
+                c0 += fmaf(-Ga, E0, Ma1 * H2 - Ma2 * H1);
+                c1 += fmaf(-Ga, E1, Ma2 * H0 - Ma0 * H2);
+                c2 += fmaf(-Ga, E2, Ma0 * H1 - Ma1 * H0);
+                const float rc = fmaf(rz, c2, fmaf(ry, c1, rx * c0));
+                const float er = fmaf(rz, E2, fmaf(ry, E1, rx * E0));
+                aG = fmaf(f, er, aG);
+                aM0 = fmaf(f, ry * H2 - rz * H1, aM0);
+                aM1 = fmaf(f, rz * H0 - rx * H2, aM1);
+                aM2 = fmaf(f, rx * H1 - ry * H0, aM2);
+                ax0 = fmaf(f, c0, ax0);
+                ax1 = fmaf(f, c1, ax1);
+                ax2 = fmaf(f, c2, ax2);
+                const float fr = f5 * rc;
+                aw0 = fmaf(fr, rx, aw0);
+                aw1 = fmaf(fr, ry, aw1);
+                aw2 = fmaf(fr, rz, aw2);
+                sp = fmaf(fr, tt, sp);
+              }
+            }
+          }
+          const float px = (float)consts[0];
+          part[0] = fmaf(-3.f, fmaf(sp, px, aw0), ax0);
+          part[1] = fmaf(-3.f, fmaf(sp, py, aw1), ax1);
+          part[2] = fmaf(-3.f, fmaf(sp, pz, aw2), ax2);
+          part[3] = aG;
+          part[4] = aM0;
+          part[5] = aM1;
+          part[6] = aM2;
+          part[7] = ap0;
+          part[8] = ap1;
+          part[9] = ap2;
+        } else {
         float SfG = 0.f, SfM0 = 0.f, SfM1 = 0.f, SfM2 = 0.f, SfE0 = 0.f, SfE1 = 0.f, SfE2 = 0.f;
         float SfH0 = 0.f, SfH1 = 0.f, SfH2 = 0.f, Sfe = 0.f, Sfh0 = 0.f, Sfh1 = 0.f, Sfh2 = 0.f;
         float aw0 = 0.f, aw1 = 0.f, aw2 = 0.f, sp = 0.f, ap0 = 0.f, ap1 = 0.f, ap2 = 0.f;
@@ -1058,7 +1127,6 @@ __global__ void __launch_bounds__(MBShape1F<NDEG>::BT, MBShape1F<NDEG>::MINB)
         // this source pair's contributions, combined in FP32
         const float xa = (float)tx, ya = (float)ty, za = (float)tz;
         const float px = (float)consts[0];
-        float part[NF];
         // gx = gE_a SfG + gB_a x SfM - Gamma_a SfE + M_a x SfH - 3 (aw + sp p)
         part[0] = fmaf(-3.f, fmaf(sp, px, aw0), gE0 * SfG + (gB1 * SfM2 - gB2 * SfM1) +
                                                     (Ma1 * SfH2 - Ma2 * SfH1) - Ga * SfE0);
@@ -1074,6 +1142,7 @@ __global__ void __launch_bounds__(MBShape1F<NDEG>::BT, MBShape1F<NDEG>::MINB)
         part[7] = ap0;
         part[8] = ap1;
         part[9] = ap2;
+        }
 #pragma unroll
         for (int q = 0; q < NF; ++q) s_acc[q * BT + tid] += (double)part[q];
       }

@@ -288,6 +288,9 @@ __global__ void __launch_bounds__(M2LShape2<NDEG>::BT)
       const bool ok = mbar_wait_bounded(&bar[bb], (uint32_t)((i >> 1) & 1), status);
       const float *G = (const float *)(smem + bb * REC);
       const double *SN = (const double *)(smem + bb * REC + MOM_BYTES);
+      // factored sums unless the two boxes nearly touch (factored_ok); at N = 2^24 the
+      // direct pairs make the M2L about 4 % slower and its error ~20x smaller
+      const bool dir = MASK || !factored_ok<M>(SN, tb, cx, cy, cz);
       if (ok) {
         for (int e = tid; e < 3 * M; e += BT) {
           const int d = e / M;
@@ -297,7 +300,7 @@ __global__ void __launch_bounds__(M2LShape2<NDEG>::BT)
           const int bi = b % M, bj = (b / M) % M, bk = b / (M * M);
           const float xb = (float)(SN[bi] - cx), yb = (float)(SN[M + bj] - cy), zb = (float)(SN[2 * M + bk] - cz);
           const float g = G[b], m0 = G[NN + b], m1 = G[2 * NN + b], m2 = G[3 * NN + b];
-          if constexpr (MASK) {
+          if (dir) {
             float4 *o = pk + 2 * b;
             o[0] = make_float4(g, g, m0, m0);
             o[1] = make_float4(m1, m1, m2, m2);
@@ -322,89 +325,97 @@ __global__ void __launch_bounds__(M2LShape2<NDEG>::BT)
             const int a0 = k, a1 = k + NP < NN ? k + NP : k;
             const double tx0 = tn[a0 % M] - cx, ty0 = tn[M + (a0 / M) % M] - cy, tz0 = tn[2 * M + a0 / (M * M)] - cz;
             const double tx1 = tn[a1 % M] - cx, ty1 = tn[M + (a1 / M) % M] - cy, tz1 = tn[2 * M + a1 / (M * M)] - cz;
-            float2 prx[M], rx2[M], ryv[M];
-            float2 rxv[MASK ? M : 1], nrxv[MASK ? M : 1];
+            // this source's sweep over its nodes (bk outer, bi inner)
+            auto sweep = [&](auto DIRECT) {
+              constexpr bool D = decltype(DIRECT)::value;
+              float2 prx[M], rx2[M], ryv[M];
+              float2 rxv[D ? M : 1], nrxv[D ? M : 1];
 #pragma unroll
-            for (int b = 0; b < M; ++b) {
-              const float2 rx = make_float2((float)(tx0 - s_sn[b]), (float)(tx1 - s_sn[b]));
-              prx[b] = mul2(px, rx);
-              rx2[b] = mul2(rx, rx);
-              ryv[b] = make_float2((float)(ty0 - s_sn[M + b]), (float)(ty1 - s_sn[M + b]));
-              if constexpr (MASK) {
-                rxv[b] = rx;
-                nrxv[b] = make_float2(-rx.x, -rx.y);
+              for (int b = 0; b < M; ++b) {
+                const float2 rx = make_float2((float)(tx0 - s_sn[b]), (float)(tx1 - s_sn[b]));
+                prx[b] = mul2(px, rx);
+                rx2[b] = mul2(rx, rx);
+                ryv[b] = make_float2((float)(ty0 - s_sn[M + b]), (float)(ty1 - s_sn[M + b]));
+                if constexpr (D) {
+                  rxv[b] = rx;
+                  nrxv[b] = make_float2(-rx.x, -rx.y);
+                }
               }
-            }
-            // factored: (G, Q, W, V) sums; masked: E and B accumulated directly
-            float2 g0 = make_float2(0.f, 0.f), q0 = g0, q1 = g0, q2 = g0, w0 = g0, w1 = g0, w2 = g0, v0 = g0,
-                   v1 = g0, v2 = g0;
+              // factored: (G, Q, W, V) sums; direct: E and B accumulated
+              float2 g0 = make_float2(0.f, 0.f), q0 = g0, q1 = g0, q2 = g0, w0 = g0, w1 = g0, w2 = g0, v0 = g0,
+                     v1 = g0, v2 = g0;
 #pragma unroll 1
-            for (int bk = 0; bk < M; ++bk) {
-              const float2 rz = make_float2((float)(tz0 - s_sn[2 * M + bk]), (float)(tz1 - s_sn[2 * M + bk]));
-              const float2 nrz = make_float2(-rz.x, -rz.y);
-              const float2 prz = mul2(pz, rz);
-              const float2 rzz = fma2(rz, rz, eps);
+              for (int bk = 0; bk < M; ++bk) {
+                const float2 rz = make_float2((float)(tz0 - s_sn[2 * M + bk]), (float)(tz1 - s_sn[2 * M + bk]));
+                const float2 nrz = make_float2(-rz.x, -rz.y);
+                const float2 prz = mul2(pz, rz);
+                const float2 rzz = fma2(rz, rz, eps);
 #pragma unroll
-              for (int bj = 0; bj < M; ++bj) {
-                const float2 ry = ryv[bj], nry = make_float2(-ry.x, -ry.y);
-                const float2 P = fma2(py, ry, prz);
-                const float2 A = fma2(ry, ry, rzz);
+                for (int bj = 0; bj < M; ++bj) {
+                  const float2 ry = ryv[bj], nry = make_float2(-ry.x, -ry.y);
+                  const float2 P = fma2(py, ry, prz);
+                  const float2 A = fma2(ry, ry, rzz);
 #pragma unroll
-                for (int bi = 0; bi < M; ++bi) {
-                  const float2 tt = add2(P, prx[bi]);
-                  const float2 d = fma2(tt, tt, add2(A, rx2[bi]));
-                  const float2 sv = rsqrt2(d);
-                  float2 s3 = mul2(mul2(sv, sv), sv);
-                  if constexpr (MASK) {
-                    s3.x = d.x > (float)kEps64 ? s3.x : 0.f;
-                    s3.y = d.y > (float)kEps64 ? s3.y : 0.f;
-                    const float4 *pb = pk + 2 * (bi + M * (bj + M * bk));
-                    const float4 e0 = pb[0], e1 = pb[1];
-                    const float2 gs = mul2(s3, lo2(e0));
-                    const float2 hx = mul2(s3, hi2(e0)), hy = mul2(s3, lo2(e1)), hz = mul2(s3, hi2(e1));
-                    g0 = fma2(gs, rxv[bi], g0);  // E
-                    q0 = fma2(gs, ry, q0);
-                    q1 = fma2(gs, rz, q1);
-                    w0 = fma2(hz, nry, fma2(hy, rz, w0));  // B = s3 M x R
-                    w1 = fma2(hx, nrz, fma2(hz, rxv[bi], w1));
-                    w2 = fma2(hy, nrxv[bi], fma2(hx, ry, w2));
-                  } else {
-                    const float4 *pb = pk + 5 * (bi + M * (bj + M * bk));
-                    const float4 e0 = pb[0], e1 = pb[1], e2 = pb[2], e3 = pb[3], e4 = pb[4];
-                    g0 = fma2(s3, lo2(e0), g0);
-                    q0 = fma2(s3, hi2(e0), q0);
-                    q1 = fma2(s3, lo2(e1), q1);
-                    q2 = fma2(s3, hi2(e1), q2);
-                    w0 = fma2(s3, lo2(e2), w0);
-                    w1 = fma2(s3, hi2(e2), w1);
-                    w2 = fma2(s3, lo2(e3), w2);
-                    v0 = fma2(s3, hi2(e3), v0);
-                    v1 = fma2(s3, lo2(e4), v1);
-                    v2 = fma2(s3, hi2(e4), v2);
+                  for (int bi = 0; bi < M; ++bi) {
+                    const float2 tt = add2(P, prx[bi]);
+                    const float2 d = fma2(tt, tt, add2(A, rx2[bi]));
+                    const float2 sv = rsqrt2(d);
+                    float2 s3 = mul2(mul2(sv, sv), sv);
+                    if constexpr (D) {
+                      if constexpr (MASK) {
+                        s3.x = d.x > (float)kEps64 ? s3.x : 0.f;
+                        s3.y = d.y > (float)kEps64 ? s3.y : 0.f;
+                      }
+                      const float4 *pb = pk + 2 * (bi + M * (bj + M * bk));
+                      const float4 e0 = pb[0], e1 = pb[1];
+                      const float2 gs = mul2(s3, lo2(e0));
+                      const float2 hx = mul2(s3, hi2(e0)), hy = mul2(s3, lo2(e1)), hz = mul2(s3, hi2(e1));
+                      g0 = fma2(gs, rxv[bi], g0);  // E
+                      q0 = fma2(gs, ry, q0);
+                      q1 = fma2(gs, rz, q1);
+                      w0 = fma2(hz, nry, fma2(hy, rz, w0));  // B = s3 M x R
+                      w1 = fma2(hx, nrz, fma2(hz, rxv[bi], w1));
+                      w2 = fma2(hy, nrxv[bi], fma2(hx, ry, w2));
+                    } else {
+                      const float4 *pb = pk + 5 * (bi + M * (bj + M * bk));
+                      const float4 e0 = pb[0], e1 = pb[1], e2 = pb[2], e3 = pb[3], e4 = pb[4];
+                      g0 = fma2(s3, lo2(e0), g0);
+                      q0 = fma2(s3, hi2(e0), q0);
+                      q1 = fma2(s3, lo2(e1), q1);
+                      q2 = fma2(s3, hi2(e1), q2);
+                      w0 = fma2(s3, lo2(e2), w0);
+                      w1 = fma2(s3, hi2(e2), w1);
+                      w2 = fma2(s3, lo2(e3), w2);
+                      v0 = fma2(s3, hi2(e3), v0);
+                      v1 = fma2(s3, lo2(e4), v1);
+                      v2 = fma2(s3, hi2(e4), v2);
+                    }
                   }
                 }
               }
-            }
-            if constexpr (MASK) {
-              // coincident nodes are admissible: the factored form would cancel catastrophically
-              fold(q, 0, g0);
-              fold(q, 1, q0);
-              fold(q, 2, q1);
-              fold(q, 3, w0);
-              fold(q, 4, w1);
-              fold(q, 5, w2);
-            } else {
-              // this source's E and B at both nodes: E = x' G - Q, B = W x x' - V, folded per
-              // source into the compensated sums
-              const float2 xa = make_float2((float)tx0, (float)tx1), ya = make_float2((float)ty0, (float)ty1),
-                           za = make_float2((float)tz0, (float)tz1);
-              fold(q, 0, sub2(mul2(xa, g0), q0));
-              fold(q, 1, sub2(mul2(ya, g0), q1));
-              fold(q, 2, sub2(mul2(za, g0), q2));
-              fold(q, 3, sub2(sub2(mul2(w1, za), mul2(w2, ya)), v0));
-              fold(q, 4, sub2(sub2(mul2(w2, xa), mul2(w0, za)), v1));
-              fold(q, 5, sub2(sub2(mul2(w0, ya), mul2(w1, xa)), v2));
-            }
+              if constexpr (D) {
+                fold(q, 0, g0);
+                fold(q, 1, q0);
+                fold(q, 2, q1);
+                fold(q, 3, w0);
+                fold(q, 4, w1);
+                fold(q, 5, w2);
+              } else {
+                // this source's E and B at both nodes: E = x' G - Q, B = W x x' - V
+                const float2 xa = make_float2((float)tx0, (float)tx1), ya = make_float2((float)ty0, (float)ty1),
+                             za = make_float2((float)tz0, (float)tz1);
+                fold(q, 0, sub2(mul2(xa, g0), q0));
+                fold(q, 1, sub2(mul2(ya, g0), q1));
+                fold(q, 2, sub2(mul2(za, g0), q2));
+                fold(q, 3, sub2(sub2(mul2(w1, za), mul2(w2, ya)), v0));
+                fold(q, 4, sub2(sub2(mul2(w2, xa), mul2(w0, za)), v1));
+                fold(q, 5, sub2(sub2(mul2(w0, ya), mul2(w1, xa)), v2));
+              }
+            };
+            if (dir)
+              sweep(std::integral_constant<bool, true>{});
+            else if constexpr (!MASK)
+              sweep(std::integral_constant<bool, false>{});
           }
         }
       }
