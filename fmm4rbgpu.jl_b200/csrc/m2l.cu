@@ -749,23 +749,93 @@ int launch_m2l_fp64(Ctx *ctx, bool accumulate) {
   return ctx->check_launch("m2l_kernel");
 }
 
+// The tensor-core kernel evaluates the factored sums only, so each target's row of the
+// M2L lists is split by factored_ok: [0] the pairs for the tensor cores, [1] the pairs
+// whose boxes nearly touch, which the CUDA-core kernel then adds with its direct sums.
+// cnt holds 2 (nc + 1) entries, the last of each half 0.
+template <int M>
+__global__ void m2l_split_count_kernel(int64_t nc, const int *__restrict__ ptr, const int *__restrict__ src,
+                                       const double *__restrict__ nodes, const double *__restrict__ bbox,
+                                       int *__restrict__ cnt) {
+  constexpr int NS = ((3 * M) + 1) & ~1;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t > nc) return;
+  int a = 0, b = 0;
+  if (t < nc) {
+    const double *tb = bbox + 6 * t;
+    const double cx = 0.5 * (tb[0] + tb[3]), cy = 0.5 * (tb[1] + tb[4]), cz = 0.5 * (tb[2] + tb[5]);
+    for (int k = ptr[t]; k < ptr[t + 1]; ++k) {
+      if (factored_ok<M>(nodes + (int64_t)src[k] * NS, tb, cx, cy, cz))
+        ++a;
+      else
+        ++b;
+    }
+  }
+  cnt[t] = a;
+  cnt[nc + 1 + t] = b;
+}
+
+template <int M>
+__global__ void m2l_split_write_kernel(int64_t nc, const int *__restrict__ ptr, const int *__restrict__ src,
+                                       const double *__restrict__ nodes, const double *__restrict__ bbox,
+                                       const int *__restrict__ ptr2, int *__restrict__ src_a, int *__restrict__ src_b) {
+  constexpr int NS = ((3 * M) + 1) & ~1;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nc) return;
+  const double *tb = bbox + 6 * t;
+  const double cx = 0.5 * (tb[0] + tb[3]), cy = 0.5 * (tb[1] + tb[4]), cz = 0.5 * (tb[2] + tb[5]);
+  int oa = ptr2[t], ob = ptr2[nc + 1 + t];
+  for (int k = ptr[t]; k < ptr[t + 1]; ++k) {
+    const int s = src[k];
+    if (factored_ok<M>(nodes + (int64_t)s * NS, tb, cx, cy, cz))
+      src_a[oa++] = s;
+    else
+      src_b[ob++] = s;
+  }
+}
+
 template <int NDEG>
 int launch_m2l_tc(Ctx *ctx, bool accumulate) {
   using S = M2LShapeTC<NDEG>;
+  constexpr int M = NDEG + 1;
+  const int64_t nc = ctx->nc;
+  if (nc <= 0) return FMMB200_OK;
+  const int *ptr = ctx->get<int>(ctx->m2l_ptr_key), *src = ctx->get<int>(ctx->m2l_src_key);
+  const double *nodes = ctx->get<double>("nodes"), *bbox = ctx->get<double>("bbox");
+  int *cnt, *ptr2, *src_a, *src_b;
+  FMM_TRY(ctx->ensure("tc_split_cnt", 2 * (nc + 1), &cnt));
+  FMM_TRY(ctx->ensure("tc_split_ptr", 2 * (nc + 1), &ptr2));
+  m2l_split_count_kernel<M><<<ceil_div(nc + 1, 256), 256, 0, ctx->stream>>>(nc, ptr, src, nodes, bbox, cnt);
+  FMM_TRY(ctx->check_launch("m2l_split_count_kernel"));
+  int64_t na = 0, nb = 0;
+  FMM_TRY(exclusive_scan_i32(ctx, cnt, ptr2, nc + 1, &na));
+  FMM_TRY(exclusive_scan_i32(ctx, cnt + nc + 1, ptr2 + nc + 1, nc + 1, &nb));
+  FMM_TRY(ctx->ensure("tc_split_src_a", na > 0 ? na : 1, &src_a));
+  FMM_TRY(ctx->ensure("tc_split_src_b", nb > 0 ? nb : 1, &src_b));
+  m2l_split_write_kernel<M><<<ceil_div(nc, 256), 256, 0, ctx->stream>>>(nc, ptr, src, nodes, bbox, ptr2, src_a,
+                                                                          src_b);
+  FMM_TRY(ctx->check_launch("m2l_split_write_kernel"));
   auto kern = m2l_tc_kernel<NDEG>;
   FMM_TRY(opt_in_smem(ctx, kern, S::SMEM));
-  if (ctx->nc > 0)
-    kern<<<(unsigned)ctx->nc, kTcThreads, S::SMEM, ctx->stream>>>(
-        ctx->get<int>(ctx->m2l_ptr_key), ctx->get<int>(ctx->m2l_src_key), ctx->get<double>("nodes"), ctx->get<double>("bbox"),
-        ctx->get<float>("mom32"), ctx->get<float>("loc32"), ctx->get<double>("consts"), accumulate ? 1 : 0,
-        ctx->d_status);
-  return ctx->check_launch("m2l_tc_kernel");
+  kern<<<(unsigned)nc, kTcThreads, S::SMEM, ctx->stream>>>(ptr2, src_a, nodes, bbox, ctx->get<float>("mom32"),
+                                                            ctx->get<float>("loc32"), ctx->get<double>("consts"),
+                                                            accumulate ? 1 : 0, ctx->d_status);
+  FMM_TRY(ctx->check_launch("m2l_tc_kernel"));
+  if (nb == 0) return FMMB200_OK;
+  using S2 = M2LShape2<NDEG>;
+  auto k2 = m2l_x2_kernel<NDEG, false>;
+  FMM_TRY(opt_in_smem(ctx, k2, S2::SMEM));
+  k2<<<(unsigned)nc, S2::BT, S2::SMEM, ctx->stream>>>(ptr2 + nc + 1, src_b, nodes, bbox, ctx->get<float>("mom32"),
+                                                      ctx->get<float>("loc32"), ctx->get<double>("consts"), 1,
+                                                      ctx->d_status);
+  return ctx->check_launch("m2l_x2_kernel");
 }
 
 template <int NDEG, bool MASK>
 int launch_m2l_mixed(Ctx *ctx, bool accumulate) {
   if constexpr (NDEG <= 4 && !MASK) {
-    // the tensor-core form is factored (E = x'G - Q): only where nodes cannot coincide
+    // the tensor-core form is factored (E = x'G - Q): only where nodes cannot coincide,
+    // and the pairs whose boxes nearly touch still go to the CUDA cores
     if (ctx->m2l_engine == FMMB200_M2L_TENSOR_CORES) return launch_m2l_tc<NDEG>(ctx, accumulate);
   }
   using S = M2LShape2<NDEG>;

@@ -79,8 +79,9 @@ int fmmb200_set_timing(fmmb200_ctx *ctx, int enable);
  * FP64 kernel).  FMMB200_M2L_AUTO (default) and FMMB200_M2L_CUDA_CORES: the
  * packed FP32x2 CUDA-core kernel.  FMMB200_M2L_TENSOR_CORES: tcgen05 TF32 MMAs
  * with hi/lo splitting for n <= 4 and eta <= 1/2 (the CUDA-core kernel
- * otherwise); same accuracy class, slower at n = 4 on B200.  The FP64 path is
- * not affected. */
+ * otherwise), on the factored sums; the source pairs whose boxes nearly touch,
+ * where factoring loses FP32 precision, still run on the CUDA cores.  Same
+ * accuracy class, slower at n = 4 on B200.  The FP64 path is not affected. */
 #define FMMB200_M2L_AUTO 0
 #define FMMB200_M2L_CUDA_CORES 1
 #define FMMB200_M2L_TENSOR_CORES 2

@@ -135,6 +135,25 @@ def test_config1_against_bruteforce(gpu_ctx, oracle_mod):
 
 
 @pytest.mark.parametrize("engine", ["auto", "tensor_cores"])
+@pytest.mark.parametrize("n", [2, 4])
+def test_mixed_on_boxes_that_nearly_touch(gpu_ctx, engine, n):
+    """A uniform beam of 2^20 particles with random momenta has admissible pairs whose boxes
+    nearly touch; the factored FP32 sums lost up to 8e-5 there (n = 2) before those pairs
+    took the direct sums.  Both engines now stay well inside 1e-5."""
+    import fmmb200
+
+    pos, _ = make("uniform", 2**20, 0)
+    mom = np.random.default_rng(5).normal(0, 0.5, (2**20, 3))
+    E, B = gpu_ctx.forward(pos, mom, fmmb200.FMMB200(n=n, N0=125, eta=0.5))
+    try:
+        gpu_ctx.set_m2l_engine(engine)
+        Em, Bm = gpu_ctx.forward(pos, mom, fmmb200.FMMB200(n=n, N0=125, eta=0.5, precision="mixed"))
+    finally:
+        gpu_ctx.set_m2l_engine("auto")
+    assert rel(Em, E) < 2e-6 and rel(Bm, B) < 2e-6, (rel(Em, E), rel(Bm, B))
+
+
+@pytest.mark.parametrize("engine", ["auto", "tensor_cores"])
 def test_mixed_matches_fp64(gpu_ctx, engine):
     import fmmb200
 
