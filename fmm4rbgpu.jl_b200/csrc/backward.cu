@@ -998,9 +998,11 @@ __global__ void __launch_bounds__(MBShape1F<NDEG>::BT, MBShape1F<NDEG>::MINB)
             const float rz = (float)(tz - s_sn[2 * M + bk]);
             const float prz = pz * rz;
             const float rzz = fmaf(rz, rz, eps);
-#pragma unroll
+            // rows one at a time: with the factored sweep's 25 unrolled evaluations the two
+            // loop bodies would not fit the instruction cache together
+#pragma unroll 1
             for (int bj = 0; bj < M; ++bj) {
-              const float ry = ryv[bj];
+              const float ry = (float)(ty - s_sn[M + bj]);
               const float P = fmaf(py, ry, prz);
               const float A = fmaf(ry, ry, rzz);
               const float4 *pb = pk + PKV * M * (bj + M * bk);
