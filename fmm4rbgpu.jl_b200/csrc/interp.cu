@@ -265,7 +265,28 @@ __global__ void __launch_bounds__(Grid<NDEG>::BT)
 // mode 0: near[q][p] += far (tree order); mode 1: out[perm[p]] = amp*(near + far).
 // Two threads per particle: h = 0 evaluates the E components, h = 1 the B
 // components of the leaf's local expansion, as three independent accumulation
-// chains over the tensor-product grid.
+// chains over the tensor-product grid.  The leaf's locals sit in shared memory
+// with each x-row padded to a whole number of 16-byte vectors, so a row of M
+// values costs ceil(M / 4) (FP32) or ceil(M / 2) (FP64) shared loads instead of M.
+__device__ __forceinline__ void unpack_vec(float4 v, float *a) {
+  a[0] = v.x;
+  a[1] = v.y;
+  a[2] = v.z;
+  a[3] = v.w;
+}
+__device__ __forceinline__ void unpack_vec(double2 v, double *a) {
+  a[0] = v.x;
+  a[1] = v.y;
+}
+
+template <typename T, int M>
+struct L2PRows {
+  static constexpr int VE = 16 / (int)sizeof(T);          // values per 16-byte load
+  static constexpr int NV = (M + VE - 1) / VE;            // loads per row
+  static constexpr int RS = NV * VE;                      // padded row stride
+  static constexpr int SMEM = 6 * M * M * RS * (int)sizeof(T);
+};
+
 template <int NDEG, bool MIXED>
 __global__ void __launch_bounds__(128)
     l2p_kernel(const int *__restrict__ leaf_ids, int leaf0, const int *__restrict__ lohi,
@@ -275,8 +296,11 @@ __global__ void __launch_bounds__(128)
   using Gd = Grid<NDEG>;
   constexpr int M = Gd::M, NN = Gd::NN, NS = Gd::NS;
   using T = typename std::conditional<MIXED, float, double>::type;
+  using V = typename std::conditional<MIXED, float4, double2>::type;
+  using Rw = L2PRows<T, M>;
+  constexpr int RS = Rw::RS, NV = Rw::NV, VE = Rw::VE;
   extern __shared__ __align__(16) unsigned char smem[];
-  T *s_loc = (T *)smem;  // 6*NN
+  T *s_loc = (T *)smem;  // [6 M M][RS]
   __shared__ double s_n64[3 * M];
   __shared__ float s_n32[3 * M];
   const int tid = threadIdx.x;
@@ -285,7 +309,10 @@ __global__ void __launch_bounds__(128)
   const int lo = lohi[2 * c], hi = lohi[2 * c + 1];
   const double *bb = bbox + 6 * (int64_t)c;
   const T *lc = (const T *)loc_v + (int64_t)c * 6 * NN;
-  for (int e = tid; e < 6 * NN; e += blockDim.x) s_loc[e] = lc[e];
+  for (int e = tid; e < 6 * M * M * RS; e += blockDim.x) {
+    const int row = e / RS, i = e - row * RS;
+    s_loc[e] = i < M ? lc[row * M + i] : T(0);
+  }
   for (int i = tid; i < 3 * M; i += blockDim.x) {
     const double v = nodes[(int64_t)c * NS + i];
     s_n64[i] = v;
@@ -293,7 +320,7 @@ __global__ void __launch_bounds__(128)
     s_n32[i] = (float)(v - 0.5 * (bb[d] + bb[3 + d]));
   }
   __syncthreads();
-  const T *L0 = s_loc + (3 * h) * NN, *L1 = L0 + NN, *L2 = L1 + NN;
+  const T *L0 = s_loc + (3 * h) * M * M * RS, *L1 = L0 + M * M * RS, *L2 = L1 + M * M * RS;
   for (int p = lo + (tid >> 1); p <= hi; p += blockDim.x >> 1) {
     T wx[M], wy[M], wz[M];
     if constexpr (MIXED) {
@@ -313,13 +340,23 @@ __global__ void __launch_bounds__(128)
       T y0 = 0, y1 = 0, y2 = 0;
 #pragma unroll
       for (int j = 0; j < M; ++j) {
-        const int o = M * (j + M * k);
+        const int o = RS * (j + M * k);
         T x0 = 0, x1 = 0, x2 = 0;
 #pragma unroll
-        for (int i = 0; i < M; ++i) {
-          x0 += wx[i] * L0[o + i];
-          x1 += wx[i] * L1[o + i];
-          x2 += wx[i] * L2[o + i];
+        for (int v = 0; v < NV; ++v) {
+          T a0[VE], a1[VE], a2[VE];
+          unpack_vec(*(const V *)(L0 + o + v * VE), a0);
+          unpack_vec(*(const V *)(L1 + o + v * VE), a1);
+          unpack_vec(*(const V *)(L2 + o + v * VE), a2);
+#pragma unroll
+          for (int u = 0; u < VE; ++u) {
+            const int i = v * VE + u;
+            if (i < M) {
+              x0 += wx[i] * a0[u];
+              x1 += wx[i] * a1[u];
+              x2 += wx[i] * a2[u];
+            }
+          }
         }
         y0 += wy[j] * x0;
         y1 += wy[j] * x1;
@@ -373,7 +410,7 @@ struct Launch {
   }
   static int l2p(Ctx *ctx, const int *ids, int64_t nleaf, int mode, double amp, double *oe, double *ob) {
     if (nleaf <= 0) return FMMB200_OK;
-    const int smem = 6 * Gd::NN * (int)sizeof(T);
+    const int smem = L2PRows<T, Gd::M>::SMEM;
     auto k = l2p_kernel<NDEG, MIXED>;
     FMM_TRY(opt_in_smem(ctx, k, smem));
     k<<<(unsigned)nleaf, 128, smem, ctx->stream>>>(

@@ -306,17 +306,16 @@ __global__ void __launch_bounds__(128) p2p_x2_kernel(const int *__restrict__ lea
           const float2 d = fma2(pr, pr, rre);
           const float2 s = rsqrt2(d);
           const float2 s3 = mul2(mul2(s, s), s);
-          const float2 gg = mul2(gam, s3);
-          e0 = fma2(gg, rx, e0);
-          e1 = fma2(gg, ry, e1);
-          e2 = fma2(gg, rz, e2);
-          const float2 hx = mul2(ux, s3), hy = mul2(uy, s3), hz = mul2(uz, s3);
-          bp0 = fma2(hy, rz, bp0);
-          bm0 = fma2(hz, ry, bm0);
-          bp1 = fma2(hz, rx, bp1);
-          bm1 = fma2(hx, rz, bm1);
-          bp2 = fma2(hx, ry, bp2);
-          bm2 = fma2(hy, rx, bm2);
+          const float2 kx = mul2(s3, rx), ky = mul2(s3, ry), kz = mul2(s3, rz);  // K = s^3 R
+          e0 = fma2(gam, kx, e0);
+          e1 = fma2(gam, ky, e1);
+          e2 = fma2(gam, kz, e2);
+          bp0 = fma2(uy, kz, bp0);  // B = u x K as (bp - bm)
+          bm0 = fma2(uz, ky, bm0);
+          bp1 = fma2(uz, kx, bp1);
+          bm1 = fma2(ux, kz, bm1);
+          bp2 = fma2(ux, ky, bp2);
+          bm2 = fma2(uy, kx, bm2);
         }
         };
         if (s_near[bb])
