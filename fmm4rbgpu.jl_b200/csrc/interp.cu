@@ -213,8 +213,8 @@ __global__ void __launch_bounds__(Grid<NDEG>::BT)
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ T L[2][3][M][M];
   T *s_par = (T *)smem;       // 6*NN
-  T *s_t1 = s_par + 6 * NN;   // 3*NN (three quantities at a time)
-  T *s_t2 = s_t1 + 3 * NN;    // 3*NN
+  T *s_t1 = s_par + 6 * NN;   // 6*NN
+  T *s_t2 = s_t1 + 6 * NN;    // 6*NN
   T *loc = (T *)loc_v;
   const int tid = threadIdx.x;
   const int p = (1 << (clevel - 1)) - 1 + blockIdx.x;
@@ -223,40 +223,38 @@ __global__ void __launch_bounds__(Grid<NDEG>::BT)
   const T *pl = loc + (int64_t)p * 6 * NN;
   for (int e = tid; e < 6 * NN; e += BT) s_par[e] = pl[e];
   __syncthreads();
+  // all six quantities per stage; the z stage of one child reads only t2, which the
+  // next child's y stage rewrites after the barrier that follows its x stage
   for (int ch = 0; ch < 2; ++ch) {
     T *cl = loc + (int64_t)(c1 + ch) * 6 * NN;
-    for (int half = 0; half < 2; ++half) {
-      const T *par = s_par + half * 3 * NN;
-      // x: t1[q][i + M(J + MK)] = sum_I Lx[i][I] par[q][I + M(J + MK)]
-      for (int e = tid; e < 3 * NN; e += BT) {
-        const int q = e / NN, o = e % NN, i = o % M, JK = o / M;
-        const T *src = par + q * NN + M * JK;
-        T v = 0;
+    // x: t1[q][i + M(J + MK)] = sum_I Lx[i][I] par[q][I + M(J + MK)]
+    for (int e = tid; e < 6 * NN; e += BT) {
+      const int i = e % M, qJK = e / M;
+      const T *src = s_par + M * qJK;
+      T v = 0;
 #pragma unroll
-        for (int I = 0; I < M; ++I) v += L[ch][0][i][I] * src[I];
-        s_t1[e] = v;
-      }
-      __syncthreads();
-      // y: t2[q][i + M(j + MK)] = sum_J Ly[j][J] t1[q][i + M(J + MK)]
-      for (int e = tid; e < 3 * NN; e += BT) {
-        const int q = e / NN, o = e % NN, i = o % M, j = (o / M) % M, K = o / (M * M);
-        const T *src = s_t1 + q * NN + i + M * M * K;
-        T v = 0;
+      for (int I = 0; I < M; ++I) v += L[ch][0][i][I] * src[I];
+      s_t1[e] = v;
+    }
+    __syncthreads();
+    // y: t2[q][i + M(j + MK)] = sum_J Ly[j][J] t1[q][i + M(J + MK)]
+    for (int e = tid; e < 6 * NN; e += BT) {
+      const int i = e % M, j = (e / M) % M, qK = e / (M * M);
+      const T *src = s_t1 + i + M * M * qK;
+      T v = 0;
 #pragma unroll
-        for (int J = 0; J < M; ++J) v += L[ch][1][j][J] * src[M * J];
-        s_t2[e] = v;
-      }
-      __syncthreads();
-      // z: child[q][i + M(j + Mk)] += sum_K Lz[k][K] t2[q][i + M(j + MK)]
-      for (int e = tid; e < 3 * NN; e += BT) {
-        const int q = e / NN, o = e % NN, ij = o % (M * M), k = o / (M * M);
-        const T *src = s_t2 + q * NN + ij;
-        T v = 0;
+      for (int J = 0; J < M; ++J) v += L[ch][1][j][J] * src[M * J];
+      s_t2[e] = v;
+    }
+    __syncthreads();
+    // z: child[q][i + M(j + Mk)] += sum_K Lz[k][K] t2[q][i + M(j + MK)]
+    for (int e = tid; e < 6 * NN; e += BT) {
+      const int q = e / NN, o = e - q * NN, ij = o % (M * M), k = o / (M * M);
+      const T *src = s_t2 + q * NN + ij;
+      T v = 0;
 #pragma unroll
-        for (int K = 0; K < M; ++K) v += L[ch][2][k][K] * src[M * M * K];
-        cl[(half * 3 + q) * NN + o] += v;
-      }
-      __syncthreads();
+      for (int K = 0; K < M; ++K) v += L[ch][2][k][K] * src[M * M * K];
+      cl[e] += v;
     }
   }
 }
@@ -401,7 +399,7 @@ struct Launch {
     return ctx->check_launch("m2m_kernel");
   }
   static int l2l(Ctx *ctx, int clevel) {
-    const int smem = 12 * Gd::NN * (int)sizeof(T);
+    const int smem = 18 * Gd::NN * (int)sizeof(T);
     auto k = l2l_kernel<NDEG, MIXED>;
     FMM_TRY(opt_in_smem(ctx, k, smem));
     k<<<1u << (clevel - 1), Gd::BT, smem, ctx->stream>>>(

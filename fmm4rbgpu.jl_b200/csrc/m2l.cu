@@ -329,17 +329,14 @@ __global__ void __launch_bounds__(M2LShape2<NDEG>::BT)
             auto sweep = [&](auto DIRECT) {
               constexpr bool D = decltype(DIRECT)::value;
               float2 prx[M], rx2[M], ryv[M];
-              float2 rxv[D ? M : 1], nrxv[D ? M : 1];
+              float2 rxv[D ? M : 1];
 #pragma unroll
               for (int b = 0; b < M; ++b) {
                 const float2 rx = make_float2((float)(tx0 - s_sn[b]), (float)(tx1 - s_sn[b]));
                 prx[b] = mul2(px, rx);
                 rx2[b] = mul2(rx, rx);
                 ryv[b] = make_float2((float)(ty0 - s_sn[M + b]), (float)(ty1 - s_sn[M + b]));
-                if constexpr (D) {
-                  rxv[b] = rx;
-                  nrxv[b] = make_float2(-rx.x, -rx.y);
-                }
+                if constexpr (D) rxv[b] = rx;
               }
               // factored: (G, Q, W, V) sums; direct: E and B accumulated
               float2 g0 = make_float2(0.f, 0.f), q0 = g0, q1 = g0, q2 = g0, w0 = g0, w1 = g0, w2 = g0, v0 = g0,
@@ -347,12 +344,11 @@ __global__ void __launch_bounds__(M2LShape2<NDEG>::BT)
 #pragma unroll 1
               for (int bk = 0; bk < M; ++bk) {
                 const float2 rz = make_float2((float)(tz0 - s_sn[2 * M + bk]), (float)(tz1 - s_sn[2 * M + bk]));
-                const float2 nrz = make_float2(-rz.x, -rz.y);
                 const float2 prz = mul2(pz, rz);
                 const float2 rzz = fma2(rz, rz, eps);
 #pragma unroll
                 for (int bj = 0; bj < M; ++bj) {
-                  const float2 ry = ryv[bj], nry = make_float2(-ry.x, -ry.y);
+                  const float2 ry = ryv[bj];
                   const float2 P = fma2(py, ry, prz);
                   const float2 A = fma2(ry, ry, rzz);
 #pragma unroll
@@ -368,14 +364,17 @@ __global__ void __launch_bounds__(M2LShape2<NDEG>::BT)
                       }
                       const float4 *pb = pk + 2 * (bi + M * (bj + M * bk));
                       const float4 e0 = pb[0], e1 = pb[1];
-                      const float2 gs = mul2(s3, lo2(e0));
-                      const float2 hx = mul2(s3, hi2(e0)), hy = mul2(s3, lo2(e1)), hz = mul2(s3, hi2(e1));
-                      g0 = fma2(gs, rxv[bi], g0);  // E
-                      q0 = fma2(gs, ry, q0);
-                      q1 = fma2(gs, rz, q1);
-                      w0 = fma2(hz, nry, fma2(hy, rz, w0));  // B = s3 M x R
-                      w1 = fma2(hx, nrz, fma2(hz, rxv[bi], w1));
-                      w2 = fma2(hy, nrxv[bi], fma2(hx, ry, w2));
+                      const float2 G = lo2(e0), M0 = hi2(e0), M1 = lo2(e1), M2 = hi2(e1);
+                      const float2 kx = mul2(s3, rxv[bi]), ky = mul2(s3, ry), kz = mul2(s3, rz);  // K
+                      g0 = fma2(G, kx, g0);  // E = G K
+                      q0 = fma2(G, ky, q0);
+                      q1 = fma2(G, kz, q1);
+                      w0 = fma2(M1, kz, w0);  // B = M x K as (w - v)
+                      v0 = fma2(M2, ky, v0);
+                      w1 = fma2(M2, kx, w1);
+                      v1 = fma2(M0, kz, v1);
+                      w2 = fma2(M0, ky, w2);
+                      v2 = fma2(M1, kx, v2);
                     } else {
                       const float4 *pb = pk + 5 * (bi + M * (bj + M * bk));
                       const float4 e0 = pb[0], e1 = pb[1], e2 = pb[2], e3 = pb[3], e4 = pb[4];
@@ -397,9 +396,9 @@ __global__ void __launch_bounds__(M2LShape2<NDEG>::BT)
                 fold(q, 0, g0);
                 fold(q, 1, q0);
                 fold(q, 2, q1);
-                fold(q, 3, w0);
-                fold(q, 4, w1);
-                fold(q, 5, w2);
+                fold(q, 3, sub2(w0, v0));
+                fold(q, 4, sub2(w1, v1));
+                fold(q, 5, sub2(w2, v2));
               } else {
                 // this source's E and B at both nodes: E = x' G - Q, B = W x x' - V
                 const float2 xa = make_float2((float)tx0, (float)tx1), ya = make_float2((float)ty0, (float)ty1),
