@@ -248,12 +248,13 @@ __global__ void __launch_bounds__(BShape<NDEG>::BT)
   using S = BShape<NDEG>;
   constexpr int M = S::M, NN = S::NN, NS = S::NS, BT = S::BT, NPT = S::NPT;
   constexpr int Q = MODE == 0 ? 6 : 4;
+  constexpr int QN = Q * NN;
   extern __shared__ __align__(16) unsigned char smem[];
-  double *s_x = (double *)smem;  // NN
-  double *s_y = s_x + NN;        // NN
-  double *s_t1 = s_y + NN;       // NN
-  double *s_t2 = s_t1 + NN;      // NN
-  double *s_e = s_t2 + NN;       // 3*NN products for the three axes
+  double *s_x = (double *)smem;  // [Q][NN]
+  double *s_y = s_x + QN;        // [Q][NN]
+  double *s_t1 = s_y + QN;       // [Q][NN]
+  double *s_t2 = s_t1 + QN;      // [Q][NN]
+  double *s_e = s_t2 + QN;       // 3*NN products for the three axes
   __shared__ double L[2][3][M][M], D[2][3][M][M];
   __shared__ double s_G[2][3][M];
   const int tid = threadIdx.x;
@@ -270,6 +271,53 @@ __global__ void __launch_bounds__(BShape<NDEG>::BT)
 #pragma unroll
     for (int q = 0; q < Q; ++q) accP[r][q] = 0.0;
   for (int e = tid; e < 2 * 3 * M; e += BT) (&s_G[0][0][0])[e] = 0.0;
+  // All Q quantities go through each contraction stage together.  A stage reads the
+  // buffer the previous one wrote and the barrier after it orders the two; the last
+  // (z) stage of a contraction reads only s_t2, which the next contraction's y stage
+  // rewrites after the barrier that follows its x stage.
+  // x stage: t1[q][i + M(J + MK)] = sum_I Wx[i][I] src[q][I + M(J + MK)]
+  auto stage_x = [&](const double(*Wx)[M], const double *src) {
+    for (int e = tid; e < QN; e += BT) {
+      const int i = e % M, qJK = e / M;
+      const double *sp = src + M * qJK;
+      double v = 0;
+#pragma unroll
+      for (int I = 0; I < M; ++I) v += Wx[i][I] * sp[I];
+      s_t1[e] = v;
+    }
+  };
+  // y stage: t2[q][i + M(j + MK)] = sum_J Wy[j][J] t1[q][i + M(J + MK)]
+  auto stage_y = [&](const double(*Wy)[M]) {
+    for (int e = tid; e < QN; e += BT) {
+      const int i = e % M, j = (e / M) % M, qK = e / (M * M);
+      const double *sp = s_t1 + i + M * M * qK;
+      double v = 0;
+#pragma unroll
+      for (int J = 0; J < M; ++J) v += Wy[j][J] * sp[M * J];
+      s_t2[e] = v;
+    }
+  };
+  // transposed x and y stages (contraction over the child index, MODE 0)
+  auto stage_xT = [&](const double(*Wx)[M], const double *src) {
+    for (int e = tid; e < QN; e += BT) {
+      const int I = e % M, qjk = e / M;
+      const double *sp = src + M * qjk;
+      double v = 0;
+#pragma unroll
+      for (int i = 0; i < M; ++i) v += Wx[i][I] * sp[i];
+      s_t1[e] = v;
+    }
+  };
+  auto stage_yT = [&](const double(*Wy)[M]) {
+    for (int e = tid; e < QN; e += BT) {
+      const int I = e % M, J = (e / M) % M, qk = e / (M * M);
+      const double *sp = s_t1 + I + M * M * qk;
+      double v = 0;
+#pragma unroll
+      for (int j = 0; j < M; ++j) v += Wy[j][J] * sp[M * j];
+      s_t2[e] = v;
+    }
+  };
   __syncthreads();
 
   for (int ch = 0; ch < 2; ++ch) {
@@ -277,106 +325,76 @@ __global__ void __launch_bounds__(BShape<NDEG>::BT)
     double eacc[NPT][3];
 #pragma unroll
     for (int r = 0; r < NPT; ++r) eacc[r][0] = eacc[r][1] = eacc[r][2] = 0.0;
-    for (int q = 0; q < Q; ++q) {
-      const double *X = (MODE == 0 ? Xfield + (int64_t)c * Q * NN : Xfield + (int64_t)c * Q * NN) + q * NN;
-      const double *Y = (MODE == 0 ? Yfield + (int64_t)p * Q * NN : Yfield + (int64_t)p * Q * NN) + q * NN;
-      for (int e = tid; e < NN; e += BT) {
+    {
+      const double *X = Xfield + (int64_t)c * QN;
+      const double *Y = Yfield + (int64_t)p * QN;
+      for (int e = tid; e < QN; e += BT) {
         s_x[e] = X[e];
         s_y[e] = Y[e];
       }
+    }
+    __syncthreads();
+    // adjoint propagation
+    if (MODE == 0) {
+      // parent[I] += sum_i W[i][I] gC[i] (contract x, y, z over the child index)
+      stage_xT(L[ch][0], s_x);
       __syncthreads();
-      // adjoint propagation
-      if (MODE == 0) {
-        // parent[I] += sum_i W[i][I] gC[i] (contract x, y, z over the child index)
-        for (int e = tid; e < NN; e += BT) {
-          const int I = e % M, jk = e / M;
-          double v = 0;
+      stage_yT(L[ch][1]);
+      __syncthreads();
 #pragma unroll
-          for (int i = 0; i < M; ++i) v += L[ch][0][i][I] * s_x[i + M * jk];
-          s_t1[e] = v;
-        }
-        __syncthreads();
-        for (int e = tid; e < NN; e += BT) {
-          const int I = e % M, J = (e / M) % M, k = e / (M * M);
-          double v = 0;
+      for (int r = 0; r < NPT; ++r) {
+        const int a = tid + r * BT;
+        if (a < NN) {
+          const int IJ = a % (M * M), K = a / (M * M);
 #pragma unroll
-          for (int j = 0; j < M; ++j) v += L[ch][1][j][J] * s_t1[I + M * j + M * M * k];
-          s_t2[e] = v;
-        }
-        __syncthreads();
-#pragma unroll
-        for (int r = 0; r < NPT; ++r) {
-          const int a = tid + r * BT;
-          if (a < NN) {
-            const int IJ = a % (M * M), K = a / (M * M);
+          for (int q = 0; q < Q; ++q) {
             double v = 0;
 #pragma unroll
-            for (int k = 0; k < M; ++k) v += L[ch][2][k][K] * s_t2[IJ + M * M * k];
+            for (int k = 0; k < M; ++k) v += L[ch][2][k][K] * s_t2[q * NN + IJ + M * M * k];
             accP[r][q] += v;
           }
         }
-        __syncthreads();
-      } else {
-        // child[i] += sum_I W[i][I] gP[I]
-        for (int e = tid; e < NN; e += BT) {
-          const int i = e % M, JK = e / M;
-          double v = 0;
-#pragma unroll
-          for (int I = 0; I < M; ++I) v += L[ch][0][i][I] * s_y[I + M * JK];
-          s_t1[e] = v;
-        }
-        __syncthreads();
-        for (int e = tid; e < NN; e += BT) {
-          const int i = e % M, j = (e / M) % M, K = e / (M * M);
-          double v = 0;
-#pragma unroll
-          for (int J = 0; J < M; ++J) v += L[ch][1][j][J] * s_t1[i + M * J + M * M * K];
-          s_t2[e] = v;
-        }
-        __syncthreads();
-        double *gc = gfield + (int64_t)c * Q * NN + q * NN;
-        for (int e = tid; e < NN; e += BT) {
-          const int ij = e % (M * M), k = e / (M * M);
-          double v = 0;
-#pragma unroll
-          for (int K = 0; K < M; ++K) v += L[ch][2][k][K] * s_t2[ij + M * M * K];
-          gc[e] += v;
-        }
-        __syncthreads();
       }
-      // geometry: e_d[a] += X[a] * (T^{(d)} Y)[a] for d = x, y, z
-      for (int d = 0; d < 3; ++d) {
-        const double(*Wx)[M] = d == 0 ? D[ch][0] : L[ch][0];
-        const double(*Wy)[M] = d == 1 ? D[ch][1] : L[ch][1];
-        const double(*Wz)[M] = d == 2 ? D[ch][2] : L[ch][2];
-        for (int e = tid; e < NN; e += BT) {
-          const int i = e % M, JK = e / M;
-          double v = 0;
+    } else {
+      // child[i] += sum_I W[i][I] gP[I]
+      stage_x(L[ch][0], s_y);
+      __syncthreads();
+      stage_y(L[ch][1]);
+      __syncthreads();
+      double *gc = gfield + (int64_t)c * QN;
+      for (int e = tid; e < QN; e += BT) {
+        const int ij = e % (M * M), qk = e / (M * M), q = qk / M, k = qk - q * M;
+        const double *sp = s_t2 + q * NN + ij;
+        double v = 0;
 #pragma unroll
-          for (int I = 0; I < M; ++I) v += Wx[i][I] * s_y[I + M * JK];
-          s_t1[e] = v;
-        }
-        __syncthreads();
-        for (int e = tid; e < NN; e += BT) {
-          const int i = e % M, j = (e / M) % M, K = e / (M * M);
-          double v = 0;
+        for (int K = 0; K < M; ++K) v += L[ch][2][k][K] * sp[M * M * K];
+        gc[e] += v;
+      }
+    }
+    // geometry: e_d[a] += sum_q X[q][a] * (T^{(d)} Y)[q][a] for d = x, y, z
+    for (int d = 0; d < 3; ++d) {
+      const double(*Wx)[M] = d == 0 ? D[ch][0] : L[ch][0];
+      const double(*Wy)[M] = d == 1 ? D[ch][1] : L[ch][1];
+      const double(*Wz)[M] = d == 2 ? D[ch][2] : L[ch][2];
+      stage_x(Wx, s_y);
+      __syncthreads();
+      stage_y(Wy);
+      __syncthreads();
 #pragma unroll
-          for (int J = 0; J < M; ++J) v += Wy[j][J] * s_t1[i + M * J + M * M * K];
-          s_t2[e] = v;
-        }
-        __syncthreads();
+      for (int r = 0; r < NPT; ++r) {
+        const int a = tid + r * BT;
+        if (a < NN) {
+          const int ij = a % (M * M), k = a / (M * M);
+          double sum = 0;
 #pragma unroll
-        for (int r = 0; r < NPT; ++r) {
-          const int a = tid + r * BT;
-          if (a < NN) {
-            const int ij = a % (M * M), k = a / (M * M);
+          for (int q = 0; q < Q; ++q) {
             double v = 0;
 #pragma unroll
-            for (int K = 0; K < M; ++K) v += Wz[k][K] * s_t2[ij + M * M * K];
-            eacc[r][d] += s_x[a] * v;
+            for (int K = 0; K < M; ++K) v += Wz[k][K] * s_t2[q * NN + ij + M * M * K];
+            sum += s_x[q * NN + a] * v;
           }
+          eacc[r][d] += sum;
         }
-        __syncthreads();
       }
     }
     // G_d[i] = sum over the nodes with index i on axis d
@@ -1625,7 +1643,7 @@ int run_backward_t(Ctx *ctx, const double *d_ge, const double *d_gb, double *d_g
   // L2L^T, children at levels ml .. 1
   {
     auto k = transfer_bwd_kernel<NDEG, 0>;
-    const int sm = 7 * NN * 8;
+    const int sm = (4 * 6 + 3) * NN * 8;
     FMM_TRY(opt_in_smem(ctx, k, sm));
     for (int l = ml; l >= 1; --l) {
       k<<<1u << (l - 1), S::BT, sm, st>>>(l - 1, nodes, bbox, ct, gloc, loc, gloc, gbox);
@@ -1669,7 +1687,7 @@ int run_backward_t(Ctx *ctx, const double *d_ge, const double *d_gb, double *d_g
   // M2M^T, parents at levels 0 .. ml-1 (top-down)
   {
     auto k = transfer_bwd_kernel<NDEG, 1>;
-    const int sm = 7 * NN * 8;
+    const int sm = (4 * 4 + 3) * NN * 8;
     FMM_TRY(opt_in_smem(ctx, k, sm));
     for (int l = 0; l < ml; ++l) {
       k<<<1u << l, S::BT, sm, st>>>(l, nodes, bbox, ct, mom, gmom, gmom, gbox);
