@@ -1448,7 +1448,7 @@ __global__ void __launch_bounds__(128)
         const float2 xl = make_float2((float)(dx0 - (double)xh.x), (float)(dx1 - (double)xh.y));
         const float2 yl = make_float2((float)(dy0 - (double)yh.x), (float)(dy1 - (double)yh.y));
         const float2 zl = make_float2((float)(dz0 - (double)zh.x), (float)(dz1 - (double)zh.y));
-        float2 gx0 = z, gx1 = z, gx2 = z, gu0 = z, gu1 = z, gu2 = z, sw = z;
+        float2 gx0 = z, gx1 = z, gx2 = z, gu0 = z, gu1 = z, gu2 = z, sw = z, ser = z;
         const float4 *S = &buf[bb][0];
         auto sweep = [&](auto FL) {
           constexpr int F = decltype(FL)::value;
@@ -1497,10 +1497,12 @@ __global__ void __launch_bounds__(128)
               gx1 = fma2(w, ry, fma2(nf, k1, gx1));
               gx2 = fma2(w, rz, fma2(nf, k2, gx2));
               sw = add2(sw, wu);
-              const float2 er = mul2(mul2(fma2(rz, e2, fma2(ry, e1, mul2(rx, e0))), nf), igp);
-              gu0 = fma2(nf, sub2(mul2(ry, h2), mul2(rz, h1)), fma2(er, up0, fma2(wu, rx, gu0)));
-              gu1 = fma2(nf, sub2(mul2(rz, h0), mul2(rx, h2)), fma2(er, up1, fma2(wu, ry, gu1)));
-              gu2 = fma2(nf, sub2(mul2(rx, h1), mul2(ry, h0)), fma2(er, up2, fma2(wu, rz, gu2)));
+              // the gamma_p = sqrt(1 + u_p.u_p) term, (u_p / gamma_p) sum -f (R.e_j), is
+              // multiplied out once per tile
+              ser = fma2(fma2(rz, e2, fma2(ry, e1, mul2(rx, e0))), nf, ser);
+              gu0 = fma2(nf, sub2(mul2(ry, h2), mul2(rz, h1)), fma2(wu, rx, gu0));
+              gu1 = fma2(nf, sub2(mul2(rz, h0), mul2(rx, h2)), fma2(wu, ry, gu1));
+              gu2 = fma2(nf, sub2(mul2(rx, h1), mul2(ry, h0)), fma2(wu, rz, gu2));
             }
           }
         };
@@ -1510,7 +1512,8 @@ __global__ void __launch_bounds__(128)
           sweep(std::integral_constant<int, 1>{});
         else if (fl == 2)
           sweep(std::integral_constant<int, 2>{});
-        const float2 part[7] = {gx0, gx1, gx2, gu0, gu1, gu2, sw};
+        const float2 sg = mul2(ser, igp);
+        const float2 part[7] = {gx0, gx1, gx2, fma2(sg, up0, gu0), fma2(sg, up1, gu1), fma2(sg, up2, gu2), sw};
 #pragma unroll
         for (int q = 0; q < 7; ++q) {
           s_acc[q][tid] += (double)part[q].x;
