@@ -394,8 +394,8 @@ def run_ours(args, world, rank, local):
     ach64 = 41.0 * st64["m2l_kernel_evals"] / (st64["ms_m2l"] * 1e-3) / 1e12 if st64["ms_m2l"] > 0 else 0.0
     kname = "m2l_tc_kernel" if (args.m2l_engine == "tensor_cores" and args.n <= 4) else "m2l_x2_kernel"
     # DRAM bytes of the packed M2L kernel per M2L pair (read + write), from an ncu capture of the
-    # same kernel on the N = 2^22 bunch (1.051e9 B for 2,557,114 pairs), scaled by this run's pairs
-    traffic = 411.1 * st["nm2l"] if kname == "m2l_x2_kernel" and args.n == 4 else None
+    # same kernel on the N = 2^22 bunch (1.056e9 B for 2,557,114 pairs), scaled by this run's pairs
+    traffic = 413.0 * st["nm2l"] if kname == "m2l_x2_kernel" and args.n == 4 else None
     roof = {"kernel": f"{kname}<{args.n}> (mixed)", "bound": "fp32", "achieved": ach32, "peak": p32.value,
             "unit": "TFLOP/s", "frac": ach32 / p32.value if p32.value else None, "traffic": traffic,
             "traffic_unit": "bytes per launch (scaled by M2L pairs from the N=2^22 capture)",
