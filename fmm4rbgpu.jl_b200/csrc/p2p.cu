@@ -14,7 +14,7 @@
 // leaf and leaves about half of them idle.
 //
 // FP64 form (p2p_kernel): 64-byte records, double arithmetic.
-// Mixed form (p2p_x2_kernel): the two targets of a lane group are evaluated in
+// Mixed form (p2p_x2_kernel): each pair of targets of a lane group is evaluated in
 // the two lanes of packed FP32x2 instructions on coordinates relative to the
 // source leaf's box centre, each stored as a hi + lo pair of floats.  Per tile
 // the targets are moved into the source's frame in FP64 once and split the same
@@ -38,6 +38,7 @@ constexpr int kP2PTile = 128;
 
 // Two target particles per lane group share every staged source record.
 constexpr int kTT = 2;
+
 
 // Number of staged tiles of target leaf c's source list (block-wide).
 __device__ __forceinline__ int count_tiles(const int *__restrict__ lohi, const int *__restrict__ src, int p0, int np,
@@ -191,7 +192,7 @@ __global__ void __launch_bounds__(128) p2p_kernel(const int *__restrict__ leaf_i
   }
 }
 
-template <int G>
+template <int G, int TP>
 __global__ void __launch_bounds__(128) p2p_x2_kernel(const int *__restrict__ leaf_ids, int leaf0,
                                                      const int *__restrict__ lohi, const int *__restrict__ ptr,
                                                      const int *__restrict__ src, const double *__restrict__ bbox,
@@ -204,7 +205,7 @@ __global__ void __launch_bounds__(128) p2p_x2_kernel(const int *__restrict__ lea
   __shared__ int s_cnt[2], s_near[2];
   __shared__ double s_centre[2][3];
   __shared__ int s_warp[33];
-  __shared__ double s_acc[12][128];  // per thread: E, B of both targets, FP64 sums over tiles
+  __shared__ double s_acc[12 * TP][128];  // per thread: E, B of its 2 TP targets, FP64 sums over tiles
 
   const int tid = threadIdx.x, BT = blockDim.x, TG = BT / G;
   const int tl = tid / G, g = tid % G;
@@ -244,15 +245,23 @@ __global__ void __launch_bounds__(128) p2p_x2_kernel(const int *__restrict__ lea
   };
 
   int it = 0;  // global iteration count (mbarrier phase parity)
-  for (int tc = 0; tc < tcnt; tc += kTT * TG) {
-    const int ti0 = tc + tl, ti1 = tc + tl + TG;
-    const bool act0 = ti0 < tcnt, act1 = ti1 < tcnt;
-    const int64_t pj0 = tlo + (act0 ? ti0 : 0), pj1 = tlo + (act1 ? ti1 : 0);
-    // FP64 target coordinates of both targets
-    const double X0 = prec64[pj0 * 8 + 0], Y0 = prec64[pj0 * 8 + 1], Z0 = prec64[pj0 * 8 + 2];
-    const double X1 = prec64[pj1 * 8 + 0], Y1 = prec64[pj1 * 8 + 1], Z1 = prec64[pj1 * 8 + 2];
+  // a lane group holds 2 TP targets: pair t = (ti[2t], ti[2t+1]) in the lanes of FP32x2
+  for (int tc = 0; tc < tcnt; tc += 2 * TP * TG) {
+    int ti[2 * TP];
+    bool act[2 * TP];
+    int64_t pj[2 * TP];
+    double tX[2 * TP], tY[2 * TP], tZ[2 * TP];  // FP64 target coordinates
 #pragma unroll
-    for (int q = 0; q < 12; ++q) s_acc[q][tid] = 0.0;
+    for (int u = 0; u < 2 * TP; ++u) {
+      ti[u] = tc + tl + u * TG;
+      act[u] = ti[u] < tcnt;
+      pj[u] = tlo + (act[u] ? ti[u] : 0);
+      tX[u] = prec64[pj[u] * 8 + 0];
+      tY[u] = prec64[pj[u] * 8 + 1];
+      tZ[u] = prec64[pj[u] * 8 + 2];
+    }
+#pragma unroll
+    for (int q = 0; q < 12 * TP; ++q) s_acc[q][tid] = 0.0;
     if (tid == 0) {
       cur = TileCursor{0, 0};
       if (W > 0) {
@@ -267,94 +276,111 @@ __global__ void __launch_bounds__(128) p2p_x2_kernel(const int *__restrict__ lea
         issue(bb ^ 1);
       }
       const bool ok = mbar_wait_bounded(&bar[bb], (uint32_t)((it >> 1) & 1), status);
-      if (ok && act0) {
+      if (ok && act[0]) {
         const int cnt = s_cnt[bb];
-        // both targets in the source leaf's frame, as hi + lo
+        // the targets in the source leaf's frame, as hi + lo
         const double scx = s_centre[bb][0], scy = s_centre[bb][1], scz = s_centre[bb][2];
-        const double dx0 = X0 - scx, dy0 = Y0 - scy, dz0 = Z0 - scz;
-        const double dx1 = X1 - scx, dy1 = Y1 - scy, dz1 = Z1 - scz;
-        const float2 xh = make_float2((float)dx0, (float)dx1), yh = make_float2((float)dy0, (float)dy1),
-                     zh = make_float2((float)dz0, (float)dz1);
-        const float2 xl = make_float2((float)(dx0 - (double)xh.x), (float)(dx1 - (double)xh.y));
-        const float2 yl = make_float2((float)(dy0 - (double)yh.x), (float)(dy1 - (double)yh.y));
-        const float2 zl = make_float2((float)(dz0 - (double)zh.x), (float)(dz1 - (double)zh.y));
+        float2 xh[TP], yh[TP], zh[TP], xl[TP], yl[TP], zl[TP];
+#pragma unroll
+        for (int t = 0; t < TP; ++t) {
+          const double dx0 = tX[2 * t] - scx, dy0 = tY[2 * t] - scy, dz0 = tZ[2 * t] - scz;
+          const double dx1 = tX[2 * t + 1] - scx, dy1 = tY[2 * t + 1] - scy, dz1 = tZ[2 * t + 1] - scz;
+          xh[t] = make_float2((float)dx0, (float)dx1);
+          yh[t] = make_float2((float)dy0, (float)dy1);
+          zh[t] = make_float2((float)dz0, (float)dz1);
+          xl[t] = make_float2((float)(dx0 - (double)xh[t].x), (float)(dx1 - (double)xh[t].y));
+          yl[t] = make_float2((float)(dy0 - (double)yh[t].x), (float)(dy1 - (double)yh[t].y));
+          zl[t] = make_float2((float)(dz0 - (double)zh[t].x), (float)(dz1 - (double)zh[t].y));
+        }
         const float2 eps = dup2((float)kEps64);
-        float2 e0 = make_float2(0.f, 0.f), e1 = e0, e2 = e0, bp0 = e0, bp1 = e0, bp2 = e0, bm0 = e0, bm1 = e0,
-               bm2 = e0;
+        const float2 z = make_float2(0.f, 0.f);
+        float2 e0[TP], e1[TP], e2[TP], bp0[TP], bp1[TP], bp2[TP], bm0[TP], bm1[TP], bm2[TP];
+#pragma unroll
+        for (int t = 0; t < TP; ++t) e0[t] = e1[t] = e2[t] = bp0[t] = bp1[t] = bp2[t] = bm0[t] = bm1[t] = bm2[t] = z;
         const float4 *S = &buf[bb][0];
         auto sweep = [&](auto NEARC) {
           constexpr bool NEAR = decltype(NEARC)::value;
 #pragma unroll 2
-        for (int j = g; j < cnt; j += G) {
-          const float4 *r = S + j * REC;
-          const float4 r0 = r[0], r1 = r[1], r3 = r[3], r4 = r[4];
-          // R = (target hi - source hi) + (target lo - source lo); the record holds -hi, -lo
-          float2 rx, ry, rz;
-          if constexpr (NEAR) {
-            const float4 r2 = r[2];
-            rx = add2(add2(xh, lo2(r0)), add2(xl, hi2(r1)));
-            ry = add2(add2(yh, hi2(r0)), add2(yl, lo2(r2)));
-            rz = add2(add2(zh, lo2(r1)), add2(zl, hi2(r2)));
-          } else {
-            rx = add2(xh, lo2(r0));
-            ry = add2(yh, hi2(r0));
-            rz = add2(zh, lo2(r1));
+          for (int j = g; j < cnt; j += G) {
+            const float4 *r = S + j * REC;
+            const float4 r0 = r[0], r1 = r[1], r3 = r[3], r4 = r[4];
+            const float4 r2 = NEAR ? r[2] : make_float4(0.f, 0.f, 0.f, 0.f);
+            const float2 gam = lo2(r3), ux = hi2(r3), uy = lo2(r4), uz = hi2(r4);
+#pragma unroll
+            for (int t = 0; t < TP; ++t) {
+              // R = (target hi - source hi) + (target lo - source lo); the record holds -hi, -lo
+              float2 rx, ry, rz;
+              if constexpr (NEAR) {
+                rx = add2(add2(xh[t], lo2(r0)), add2(xl[t], hi2(r1)));
+                ry = add2(add2(yh[t], hi2(r0)), add2(yl[t], lo2(r2)));
+                rz = add2(add2(zh[t], lo2(r1)), add2(zl[t], hi2(r2)));
+              } else {
+                rx = add2(xh[t], lo2(r0));
+                ry = add2(yh[t], hi2(r0));
+                rz = add2(zh[t], lo2(r1));
+              }
+              const float2 rre = fma2(rx, rx, fma2(ry, ry, fma2(rz, rz, eps)));
+              const float2 pr = fma2(uz, rz, fma2(uy, ry, mul2(ux, rx)));
+              const float2 d = fma2(pr, pr, rre);
+              const float2 s = rsqrt2(d);
+              const float2 s3 = mul2(mul2(s, s), s);
+              const float2 kx = mul2(s3, rx), ky = mul2(s3, ry), kz = mul2(s3, rz);  // K = s^3 R
+              e0[t] = fma2(gam, kx, e0[t]);
+              e1[t] = fma2(gam, ky, e1[t]);
+              e2[t] = fma2(gam, kz, e2[t]);
+              bp0[t] = fma2(uy, kz, bp0[t]);  // B = u x K as (bp - bm)
+              bm0[t] = fma2(uz, ky, bm0[t]);
+              bp1[t] = fma2(uz, kx, bp1[t]);
+              bm1[t] = fma2(ux, kz, bm1[t]);
+              bp2[t] = fma2(ux, ky, bp2[t]);
+              bm2[t] = fma2(uy, kx, bm2[t]);
+            }
           }
-          const float2 gam = lo2(r3), ux = hi2(r3), uy = lo2(r4), uz = hi2(r4);
-          const float2 rre = fma2(rx, rx, fma2(ry, ry, fma2(rz, rz, eps)));
-          const float2 pr = fma2(uz, rz, fma2(uy, ry, mul2(ux, rx)));
-          const float2 d = fma2(pr, pr, rre);
-          const float2 s = rsqrt2(d);
-          const float2 s3 = mul2(mul2(s, s), s);
-          const float2 kx = mul2(s3, rx), ky = mul2(s3, ry), kz = mul2(s3, rz);  // K = s^3 R
-          e0 = fma2(gam, kx, e0);
-          e1 = fma2(gam, ky, e1);
-          e2 = fma2(gam, kz, e2);
-          bp0 = fma2(uy, kz, bp0);  // B = u x K as (bp - bm)
-          bm0 = fma2(uz, ky, bm0);
-          bp1 = fma2(uz, kx, bp1);
-          bm1 = fma2(ux, kz, bm1);
-          bp2 = fma2(ux, ky, bp2);
-          bm2 = fma2(uy, kx, bm2);
-        }
         };
         if (s_near[bb])
           sweep(std::integral_constant<bool, true>{});
         else
           sweep(std::integral_constant<bool, false>{});
-        const float2 part[6] = {e0, e1, e2, sub2(bp0, bm0), sub2(bp1, bm1), sub2(bp2, bm2)};
 #pragma unroll
-        for (int q = 0; q < 6; ++q) {
-          s_acc[q][tid] += (double)part[q].x;
-          s_acc[6 + q][tid] += (double)part[q].y;
+        for (int t = 0; t < TP; ++t) {
+          const float2 part[6] = {e0[t], e1[t], e2[t], sub2(bp0[t], bm0[t]), sub2(bp1[t], bm1[t]),
+                                  sub2(bp2[t], bm2[t])};
+#pragma unroll
+          for (int q = 0; q < 6; ++q) {
+            s_acc[12 * t + q][tid] += (double)part[q].x;
+            s_acc[12 * t + 6 + q][tid] += (double)part[q].y;
+          }
         }
       }
       __syncthreads();  // buffer bb is refilled two iterations later
     }
     // combine the G lanes of each target group (warp shuffles), FP64 result
-    double v0[6], v1[6];
 #pragma unroll
-    for (int q = 0; q < 6; ++q) {
-      v0[q] = s_acc[q][tid];
-      v1[q] = s_acc[6 + q][tid];
-#pragma unroll
-      for (int o = 1; o < G; o <<= 1) {
-        v0[q] += __shfl_xor_sync(0xffffffffu, v0[q], o);
-        v1[q] += __shfl_xor_sync(0xffffffffu, v1[q], o);
-      }
-    }
-    if (g == 0) {
+    for (int t = 0; t < TP; ++t) {
+      double v0[6], v1[6];
 #pragma unroll
       for (int q = 0; q < 6; ++q) {
-        if (act0) {
-          double o = v0[q];
-          if (accumulate) o += near[(int64_t)q * N + pj0];
-          near[(int64_t)q * N + pj0] = o;
+        v0[q] = s_acc[12 * t + q][tid];
+        v1[q] = s_acc[12 * t + 6 + q][tid];
+#pragma unroll
+        for (int o = 1; o < G; o <<= 1) {
+          v0[q] += __shfl_xor_sync(0xffffffffu, v0[q], o);
+          v1[q] += __shfl_xor_sync(0xffffffffu, v1[q], o);
         }
-        if (act1) {
-          double o = v1[q];
-          if (accumulate) o += near[(int64_t)q * N + pj1];
-          near[(int64_t)q * N + pj1] = o;
+      }
+      if (g == 0) {
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+          if (act[2 * t]) {
+            double o = v0[q];
+            if (accumulate) o += near[(int64_t)q * N + pj[2 * t]];
+            near[(int64_t)q * N + pj[2 * t]] = o;
+          }
+          if (act[2 * t + 1]) {
+            double o = v1[q];
+            if (accumulate) o += near[(int64_t)q * N + pj[2 * t + 1]];
+            near[(int64_t)q * N + pj[2 * t + 1]] = o;
+          }
         }
       }
     }
@@ -371,10 +397,15 @@ int launch_p2p_fp64(Ctx *ctx, const int *d_leaf_ids, int64_t nleaf, bool accumul
   return ctx->check_launch("p2p_kernel");
 }
 
+// Leaves above 128 particles (G = 1): two target pairs per lane group over two lanes, which
+// halves the shared loads per evaluation (beamlets, N0 = 200: 44.1 -> 37.4 ms at 2^22); for
+// smaller leaves one pair per group keeps the register count at 80 and is faster.
 template <int G>
 int launch_p2p_mixed(Ctx *ctx, const int *d_leaf_ids, int64_t nleaf, bool accumulate) {
   if (nleaf <= 0) return FMMB200_OK;
-  p2p_x2_kernel<G><<<(unsigned)nleaf, 128, 0, ctx->stream>>>(
+  constexpr int TP = G == 1 ? 2 : 1;
+  constexpr int GG = G * TP;
+  p2p_x2_kernel<GG, TP><<<(unsigned)nleaf, 128, 0, ctx->stream>>>(
       d_leaf_ids, (int)ctx->leaf0, ctx->get<int>("lohi"), ctx->get<int>("p2p_ptr"), ctx->get<int>("p2p_src"),
       ctx->get<double>("bbox"), ctx->get<float4>("prec32x2"), ctx->get<double>("prec64"), ctx->get<double>("near"),
       (int)ctx->N, accumulate ? 1 : 0, ctx->d_status);
