@@ -118,71 +118,97 @@ __global__ void __launch_bounds__(128)
   for (int i = tid; i < 3 * M; i += blockDim.x) s_n[i] = nodes[(int64_t)c * NS + i];
   __syncthreads();
   double gbx[6] = {0, 0, 0, 0, 0, 0};
-  for (int p = lo + tid; p <= hi; p += blockDim.x) {
-    const double *r = prec + 8 * (int64_t)p;
+  // Two threads per particle (h = tid & 1), each over half of the Q quantities.  The
+  // position gradient is linear in the fields, so each thread folds its quantities
+  // into one field first (by the particle's adjoint a_q, or by (gamma, u) for P2M^T)
+  // and contracts that once with the weights and their derivatives; a shuffle adds the
+  // two halves.
+  constexpr int QH = Q / 2;
+  const int h = tid & 1;
+  for (int base = lo; base <= hi; base += (int)blockDim.x / 2) {
+    const int p = base + (tid >> 1);
+    const bool act = p <= hi;
+    const double *r = prec + 8 * (int64_t)(act ? p : lo);
     double w[3][M], dw[3][M];
     weights_d64<M>(r[0], s_n, w[0], dw[0]);
     weights_d64<M>(r[1], s_n + M, w[1], dw[1]);
     weights_d64<M>(r[2], s_n + 2 * M, w[2], dw[2]);
-    double I[Q], D[3][Q];
-#pragma unroll
-    for (int q = 0; q < Q; ++q) {
-      const double *F = s_f + q * NN;
-      double vi = 0, dx = 0, dy = 0, dz = 0;
-      for (int k = 0; k < M; ++k) {
-        double ay = 0, ady = 0, axd = 0;
-#pragma unroll
-        for (int j = 0; j < M; ++j) {
-          const double *row = F + M * (j + M * k);
-          double vx = 0, vdx = 0;
-#pragma unroll
-          for (int i = 0; i < M; ++i) {
-            vx += w[0][i] * row[i];
-            vdx += dw[0][i] * row[i];
-          }
-          ay += w[1][j] * vx;
-          ady += dw[1][j] * vx;
-          axd += w[1][j] * vdx;
-        }
-        vi += w[2][k] * ay;
-        dx += w[2][k] * axd;
-        dy += w[2][k] * ady;
-        dz += dw[2][k] * ay;
-      }
-      I[q] = vi;
-      D[0][q] = dx;
-      D[1][q] = dy;
-      D[2][q] = dz;
-    }
-    double G[3];
+    // this thread's fold coefficients and, for P2M^T, the values of its quantities
+    double cq[QH];
     if (MODE == 0) {
-      double a[6];
 #pragma unroll
-      for (int q = 0; q < 6; ++q) a[q] = adj[(int64_t)q * N + p];
+      for (int u = 0; u < QH; ++u) cq[u] = act ? adj[(int64_t)(QH * h + u) * N + p] : 0.0;
+    } else {
+      const double cf[4] = {r[3], r[4], r[5], r[6]};  // gamma, u
+#pragma unroll
+      for (int u = 0; u < QH; ++u) cq[u] = act ? cf[QH * h + u] : 0.0;
+    }
+    double Iv[QH];
+#pragma unroll
+    for (int u = 0; u < QH; ++u) Iv[u] = 0.0;
+    double dx = 0, dy = 0, dz = 0;
+#pragma unroll
+    for (int k = 0; k < M; ++k) {
+      double ay = 0, ady = 0, axd = 0, iy[QH];
+#pragma unroll
+      for (int u = 0; u < QH; ++u) iy[u] = 0.0;
+#pragma unroll
+      for (int j = 0; j < M; ++j) {
+        const double *row = s_f + (QH * h) * NN + M * (j + M * k);
+        double vx = 0, vdx = 0, ix[QH];
+#pragma unroll
+        for (int u = 0; u < QH; ++u) ix[u] = 0.0;
+#pragma unroll
+        for (int i = 0; i < M; ++i) {
+          double hv = 0;
+#pragma unroll
+          for (int u = 0; u < QH; ++u) {
+            const double f = row[u * NN + i];
+            hv += cq[u] * f;
+            if (MODE == 1) ix[u] += w[0][i] * f;
+          }
+          vx += w[0][i] * hv;
+          vdx += dw[0][i] * hv;
+        }
+        ay += w[1][j] * vx;
+        ady += dw[1][j] * vx;
+        axd += w[1][j] * vdx;
+        if (MODE == 1)
+#pragma unroll
+          for (int u = 0; u < QH; ++u) iy[u] += w[1][j] * ix[u];
+      }
+      dx += w[2][k] * axd;
+      dy += w[2][k] * ady;
+      dz += dw[2][k] * ay;
+      if (MODE == 1)
+#pragma unroll
+        for (int u = 0; u < QH; ++u) Iv[u] += w[2][k] * iy[u];
+    }
+    double G[3] = {dx, dy, dz};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) G[d] += __shfl_xor_sync(0xffffffffu, G[d], 1);
+    if (MODE == 1) {
+      // gu += I_M + (I_Gamma / gamma) u: thread 0 holds I_Gamma, I_M0; thread 1 I_M1, I_M2
+      const double ig = __shfl_sync(0xffffffffu, Iv[0], (tid & 31) & ~1) / r[3];
+      if (act) {
+        if (h == 0) {
+          gxu[(int64_t)3 * N + p] += Iv[1] + ig * r[4];
+        } else {
+          gxu[(int64_t)4 * N + p] += Iv[0] + ig * r[5];
+          gxu[(int64_t)5 * N + p] += Iv[1] + ig * r[6];
+        }
+      }
+    }
+    if (act && h == 0) {
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
-        double g = 0;
-#pragma unroll
-        for (int q = 0; q < 6; ++q) g += a[q] * D[d][q];
-        G[d] = g;
-      }
-    } else {
-      const double gam = r[3], ux = r[4], uy = r[5], uz = r[6];
-#pragma unroll
-      for (int d = 0; d < 3; ++d) G[d] = gam * D[d][0] + ux * D[d][1] + uy * D[d][2] + uz * D[d][3];
-      const double ig = I[0] / gam;
-      gxu[(int64_t)3 * N + p] += I[1] + ig * ux;
-      gxu[(int64_t)4 * N + p] += I[2] + ig * uy;
-      gxu[(int64_t)5 * N + p] += I[3] + ig * uz;
-    }
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      gxu[(int64_t)d * N + p] += G[d];
-      const double a = bb[d], b = bb[3 + d], wd = b - a;
-      if (wd > 0.0) {
-        const double xi = (r[d] - a) / wd;
-        gbx[d] += (xi - 1.0) * G[d];
-        gbx[3 + d] += -xi * G[d];
+        gxu[(int64_t)d * N + p] += G[d];
+        const double a = bb[d], b = bb[3 + d], wd = b - a;
+        if (wd > 0.0) {
+          const double xi = (r[d] - a) / wd;
+          gbx[d] += (xi - 1.0) * G[d];
+          gbx[3 + d] += -xi * G[d];
+        }
       }
     }
   }
