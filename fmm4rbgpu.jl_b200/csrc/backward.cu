@@ -817,7 +817,7 @@ __global__ void __launch_bounds__(MBShape2<NDEG>::BT)
                   sv.y = d.y > epsf ? sv.y : 0.f;
                 }
                 const float2 s2 = mul2(sv, sv);
-                const float2 f = mul2(s2, sv), f5 = mul2(f, s2);
+                const float2 f = mul2(s2, sv);  // the s^5 terms are formed as f (s^2 ...): no FP32 overflow
                 float2 c0 = z, c1 = z, c2 = z, rc = z;
                 if constexpr ((F & 1) != 0) {
                   const float4 q0 = pb[5 * bi], q1 = pb[5 * bi + 1];
@@ -826,7 +826,7 @@ __global__ void __launch_bounds__(MBShape2<NDEG>::BT)
                   c1 = fma2(Gb, gE1, fma2(gB2, Mb0, mul2(ngB0, Mb2)));
                   c2 = fma2(Gb, gE2, fma2(gB0, Mb1, mul2(ngB1, Mb0)));
                   rc = fma2(rz, c2, fma2(ry, c1, mul2(rx, c0)));
-                  const float2 w1 = mul2(mul2(f5, tt), rc);
+                  const float2 w1 = mul2(f, mul2(mul2(s2, tt), rc));
                   ap0 = fma2(w1, rx, ap0);
                   ap1 = fma2(w1, ry, ap1);
                   ap2 = fma2(w1, rz, ap2);
@@ -844,7 +844,7 @@ __global__ void __launch_bounds__(MBShape2<NDEG>::BT)
                   aM1 = fma2(f, fma2(rz, H0, mul2(nrxv[bi], H2)), aM1);
                   aM2 = fma2(f, fma2(rx, H1, mul2(nry, H0)), aM2);
                 }
-                const float2 fr = mul2(f5, rc);
+                const float2 fr = mul2(f, mul2(s2, rc));
                 axf0 = fma2(f, c0, axf0);
                 axf1 = fma2(f, c1, axf1);
                 axf2 = fma2(f, c2, axf2);
@@ -1057,7 +1057,7 @@ __global__ void __launch_bounds__(MBShape1F<NDEG>::BT, MBShape1F<NDEG>::MINB)
                 const float d = fmaf(tt, tt, A + rx2[bi]);
                 const float sv = rsqrt_approx_f32(d);
                 const float s2 = sv * sv;
-                const float f = s2 * sv, f5 = f * s2;
+                const float f = s2 * sv;  // the s^5 terms are formed as f (s^2 ...): no FP32 overflow
                 const float4 q0 = pb[PKV * bi], q1 = pb[PKV * bi + 1];
                 const float2 q2 = *(const float2 *)(pb + PKV * bi + 2);
                 const float Gb = q0.x, Mb0 = q0.y, Mb1 = q0.z, Mb2 = q0.w;
@@ -1066,7 +1066,7 @@ __global__ void __launch_bounds__(MBShape1F<NDEG>::BT, MBShape1F<NDEG>::MINB)
                 float c1 = fmaf(Gb, gE1, gB2 * Mb0 - gB0 * Mb2);
                 float c2 = fmaf(Gb, gE2, gB0 * Mb1 - gB1 * Mb0);
                 const float rc1 = fmaf(rz, c2, fmaf(ry, c1, rx * c0));
-                const float wp = (f5 * tt) * rc1;
+                const float wp = f * ((s2 * tt) * rc1);
                 ap0 = fmaf(wp, rx, ap0);
                 ap1 = fmaf(wp, ry, ap1);
                 ap2 = fmaf(wp, rz, ap2);
@@ -1082,7 +1082,7 @@ __global__ void __launch_bounds__(MBShape1F<NDEG>::BT, MBShape1F<NDEG>::MINB)
                 ax0 = fmaf(f, c0, ax0);
                 ax1 = fmaf(f, c1, ax1);
                 ax2 = fmaf(f, c2, ax2);
-                const float fr = f5 * rc;
+                const float fr = f * (s2 * rc);
                 aw0 = fmaf(fr, rx, aw0);
                 aw1 = fmaf(fr, ry, aw1);
                 aw2 = fmaf(fr, rz, aw2);
@@ -1131,7 +1131,7 @@ __global__ void __launch_bounds__(MBShape1F<NDEG>::BT, MBShape1F<NDEG>::MINB)
               const float d = fmaf(tt, tt, A + rx2[bi]);
               const float sv = rsqrt_approx_f32(d);
               const float s2 = sv * sv;
-              const float f = s2 * sv, f5 = f * s2;
+              const float f = s2 * sv;  // the s^5 terms are formed as f (s^2 ...): no FP32 overflow
               const float4 q0 = pb[PKV * bi], q1 = pb[PKV * bi + 1], q2 = pb[PKV * bi + 2];
               const float2 q3 = *(const float2 *)(pb + PKV * bi + 3);
               const float Gb = q0.x, Mb0 = q0.y, Mb1 = q0.z, Mb2 = q0.w;
@@ -1144,11 +1144,11 @@ __global__ void __launch_bounds__(MBShape1F<NDEG>::BT, MBShape1F<NDEG>::MINB)
               const float v1 = fmaf(rx, -Ma2, v1k);
               const float v2 = fmaf(rx, Ma1, v2j);
               const float rc = fmaf(H2, v2, fmaf(H1, v1, fmaf(H0, v0, fmaf(-Ga, er, rc1))));
-              const float wp = (f5 * tt) * rc1;
+              const float wp = f * ((s2 * tt) * rc1);
               ap0 = fmaf(wp, rx, ap0);
               ap1 = fmaf(wp, ry, ap1);
               ap2 = fmaf(wp, rz, ap2);
-              const float fr = f5 * rc;
+              const float fr = f * (s2 * rc);
               aw0 = fmaf(fr, rx, aw0);
               aw1 = fmaf(fr, ry, aw1);
               aw2 = fmaf(fr, rz, aw2);

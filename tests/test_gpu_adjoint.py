@@ -196,3 +196,74 @@ def test_backward_without_saved_forward_is_an_error(gpu_ctx):
         ctx.backward(np.zeros_like(pos), np.zeros_like(pos))
     assert ei.value.status == fmmb200.ERR_NO_STATE
     ctx.close()
+
+
+@pytest.mark.parametrize("eta", [0.5, 0.6])
+def test_mixed_adjoint_on_a_line_stays_finite(gpu_ctx, eta):
+    """Half a million particles on a line: the boxes are flat in y and z, and neighbouring
+    boxes' end nodes can lie ~1e-12 apart, where s^5 = d^-5/2 exceeds the FP32 range.  The
+    mixed adjoint forms those terms as f (s^2 ...) and stays finite and within 1e-4 of FP64
+    (it returned NaN for eta = 0.6 before)."""
+    import fmmb200
+    from fmmb200 import beams
+
+    N = 500000
+    pos, _ = beams.uniform(N, seed=16)
+    pos[:, 1] = 0.2
+    pos[:, 2] = 0.7
+    mom = np.random.default_rng(16).normal(0, 0.5, (N, 3))
+    rng = np.random.default_rng(3)
+    w = rng.normal(size=(N, 3))
+    v = rng.normal(size=(N, 3))
+    _, gx, gu = fmm_loss_grad(gpu_ctx, pos, mom, fmmb200.FMMB200(n=1, N0=64, eta=eta), w, v)
+    _, gxm, gum = fmm_loss_grad(gpu_ctx, pos, mom, fmmb200.FMMB200(n=1, N0=64, eta=eta, precision="mixed"), w, v)
+    assert np.all(np.isfinite(gxm)) and np.all(np.isfinite(gum))
+    assert rel(gxm, gx) < 1e-4 and rel(gum, gu) < 1e-4, (rel(gxm, gx), rel(gum, gu))
+
+
+def _random_case(k):
+    rng = np.random.default_rng(1000 + k)
+    N = int(rng.choice([20000, 100000, 300000]))
+    n = int(rng.integers(1, 9))
+    N0 = int(rng.choice([16, 40, 64, 125, 200, 400]))
+    eta = float(rng.choice([0.3, 0.5, 0.6, 0.7]))
+    dist = str(rng.choice(["gauss", "uniform", "beamlets", "planar", "line"]))
+    return N, n, N0, eta, dist
+
+
+@pytest.mark.parametrize("k", range(12))
+def test_random_configurations_mixed_vs_fp64(gpu_ctx, k):
+    """Seeded random (N, n, N0, eta, distribution) cases, degenerate planar and collinear
+    beams included: the mixed forward within 1e-5 and its adjoint within 1e-4 of FP64,
+    every value finite."""
+    import fmmb200
+    from fmmb200 import beams
+
+    N, n, N0, eta, dist = _random_case(k)
+    if dist == "gauss":
+        pos, mom = beams.gaussian_bunch(N, seed=k)
+    elif dist == "beamlets":
+        pos, mom = beams.beamlets(N, seed=k)
+    else:
+        pos, _ = beams.uniform(N, seed=k)
+        mom = np.random.default_rng(k).normal(0, 0.5, (N, 3))
+        if dist == "planar":
+            pos[:, 2] = 0.3
+        elif dist == "line":
+            pos[:, 1] = 0.2
+            pos[:, 2] = 0.7
+    rng = np.random.default_rng(k + 7)
+    w = rng.normal(size=(N, 3))
+    v = rng.normal(size=(N, 3))
+    res = {}
+    for prec in ("fp64", "mixed"):
+        alg = fmmb200.FMMB200(n=n, N0=N0, eta=eta, precision=prec)
+        E, B = gpu_ctx.forward(pos, mom, alg, save_for_backward=True)
+        gx, gu = gpu_ctx.backward(w, v)
+        res[prec] = (E, B, gx, gu)
+    for a in res["mixed"]:
+        assert np.all(np.isfinite(a))
+    (E, B, gx, gu), (Em, Bm, gxm, gum) = res["fp64"], res["mixed"]
+    case = (N, n, N0, eta, dist)
+    assert rel(Em, E) < 1e-5 and rel(Bm, B) < 1e-5, (case, rel(Em, E), rel(Bm, B))
+    assert rel(gxm, gx) < 1e-4 and rel(gum, gu) < 1e-4, (case, rel(gxm, gx), rel(gum, gu))
