@@ -1033,22 +1033,32 @@ __global__ void __launch_bounds__(MBShape1F<NDEG>::BT, MBShape1F<NDEG>::MINB)
         }
         float part[NF];
         if (!factored_ok<M>(SN, tb, cx, cy, cz)) {
-          // boxes that nearly touch: the unfactored sums of m2l_bwd_x2_kernel
-          //   c = Gamma_b gE_a + gB_a x M_b - Gamma_a gE_b + M_a x gB_b,  c1 its first two terms
-          float ax0 = 0.f, ax1 = 0.f, ax2 = 0.f, aG = 0.f, aM0 = 0.f, aM1 = 0.f, aM2 = 0.f;
+          // Boxes that nearly touch: the factored form of the moment adjoints, x_a . SfE - Sfe
+          // and x_a x SfH - Sfh, would cancel, so those two sums are accumulated directly
+          // (f R.gE_b, f R x gB_b); the other sums have no position difference and stay
+          // factored.  Rows one at a time: with the factored branch's 25 unrolled evaluations
+          // the two loop bodies would not fit the instruction cache together.
+          float SfG = 0.f, SfM0 = 0.f, SfM1 = 0.f, SfM2 = 0.f, SfE0 = 0.f, SfE1 = 0.f, SfE2 = 0.f;
+          float SfH0 = 0.f, SfH1 = 0.f, SfH2 = 0.f, aG = 0.f, aM0 = 0.f, aM1 = 0.f, aM2 = 0.f;
           float aw0 = 0.f, aw1 = 0.f, aw2 = 0.f, sp = 0.f, ap0 = 0.f, ap1 = 0.f, ap2 = 0.f;
 #pragma unroll 1
           for (int bk = 0; bk < M; ++bk) {
             const float rz = (float)(tz - s_sn[2 * M + bk]);
             const float prz = pz * rz;
             const float rzz = fmaf(rz, rz, eps);
-            // rows one at a time: with the factored sweep's 25 unrolled evaluations the two
-            // loop bodies would not fit the instruction cache together
+            const float ek = rz * gE2;
+            const float w1k = rz * gB0;
+            const float v1k = rz * Ma0;
 #pragma unroll 1
             for (int bj = 0; bj < M; ++bj) {
               const float ry = (float)(ty - s_sn[M + bj]);
               const float P = fmaf(py, ry, prz);
               const float A = fmaf(ry, ry, rzz);
+              const float ejk = fmaf(ry, gE1, ek);
+              const float w0 = fmaf(ry, gB2, -(rz * gB1));
+              const float w2j = -(ry * gB0);
+              const float v0 = fmaf(ry, Ma2, -(rz * Ma1));
+              const float v2j = -(ry * Ma0);
               const float4 *pb = pk + PKV * M * (bj + M * bk);
 #pragma unroll
               for (int bi = 0; bi < M; ++bi) {
@@ -1062,38 +1072,47 @@ __global__ void __launch_bounds__(MBShape1F<NDEG>::BT, MBShape1F<NDEG>::MINB)
                 const float2 q2 = *(const float2 *)(pb + PKV * bi + 2);
                 const float Gb = q0.x, Mb0 = q0.y, Mb1 = q0.z, Mb2 = q0.w;
                 const float E0 = q1.x, E1 = q1.y, E2 = q1.z, H0 = q1.w, H1 = q2.x, H2 = q2.y;
-                float c0 = fmaf(Gb, gE0, gB1 * Mb2 - gB2 * Mb1);
-                float c1 = fmaf(Gb, gE1, gB2 * Mb0 - gB0 * Mb2);
-                float c2 = fmaf(Gb, gE2, gB0 * Mb1 - gB1 * Mb0);
-                const float rc1 = fmaf(rz, c2, fmaf(ry, c1, rx * c0));
+                const float rge = fmaf(rx, gE0, ejk);
+                const float w1 = fmaf(rx, -gB2, w1k);
+                const float w2 = fmaf(rx, gB1, w2j);
+                const float rc1 = fmaf(Gb, rge, fmaf(Mb2, w2, fmaf(Mb1, w1, Mb0 * w0)));
+                const float er = fmaf(rz, E2, fmaf(ry, E1, rx * E0));
+                const float v1 = fmaf(rx, -Ma2, v1k);
+                const float v2 = fmaf(rx, Ma1, v2j);
+                const float rc = fmaf(H2, v2, fmaf(H1, v1, fmaf(H0, v0, fmaf(-Ga, er, rc1))));
                 const float wp = f * ((s2 * tt) * rc1);
                 ap0 = fmaf(wp, rx, ap0);
                 ap1 = fmaf(wp, ry, ap1);
                 ap2 = fmaf(wp, rz, ap2);
-                c0 += fmaf(-Ga, E0, Ma1 * H2 - Ma2 * H1);
-                c1 += fmaf(-Ga, E1, Ma2 * H0 - Ma0 * H2);
-                c2 += fmaf(-Ga, E2, Ma0 * H1 - Ma1 * H0);
-                const float rc = fmaf(rz, c2, fmaf(ry, c1, rx * c0));
-                const float er = fmaf(rz, E2, fmaf(ry, E1, rx * E0));
-                aG = fmaf(f, er, aG);
-                aM0 = fmaf(f, ry * H2 - rz * H1, aM0);
-                aM1 = fmaf(f, rz * H0 - rx * H2, aM1);
-                aM2 = fmaf(f, rx * H1 - ry * H0, aM2);
-                ax0 = fmaf(f, c0, ax0);
-                ax1 = fmaf(f, c1, ax1);
-                ax2 = fmaf(f, c2, ax2);
                 const float fr = f * (s2 * rc);
                 aw0 = fmaf(fr, rx, aw0);
                 aw1 = fmaf(fr, ry, aw1);
                 aw2 = fmaf(fr, rz, aw2);
                 sp = fmaf(fr, tt, sp);
+                SfG = fmaf(f, Gb, SfG);
+                SfM0 = fmaf(f, Mb0, SfM0);
+                SfM1 = fmaf(f, Mb1, SfM1);
+                SfM2 = fmaf(f, Mb2, SfM2);
+                SfE0 = fmaf(f, E0, SfE0);
+                SfE1 = fmaf(f, E1, SfE1);
+                SfE2 = fmaf(f, E2, SfE2);
+                SfH0 = fmaf(f, H0, SfH0);
+                SfH1 = fmaf(f, H1, SfH1);
+                SfH2 = fmaf(f, H2, SfH2);
+                aG = fmaf(f, er, aG);
+                aM0 = fmaf(f, fmaf(ry, H2, -(rz * H1)), aM0);
+                aM1 = fmaf(f, fmaf(rz, H0, -(rx * H2)), aM1);
+                aM2 = fmaf(f, fmaf(rx, H1, -(ry * H0)), aM2);
               }
             }
           }
           const float px = (float)consts[0];
-          part[0] = fmaf(-3.f, fmaf(sp, px, aw0), ax0);
-          part[1] = fmaf(-3.f, fmaf(sp, py, aw1), ax1);
-          part[2] = fmaf(-3.f, fmaf(sp, pz, aw2), ax2);
+          part[0] = fmaf(-3.f, fmaf(sp, px, aw0), gE0 * SfG + (gB1 * SfM2 - gB2 * SfM1) +
+                                                      (Ma1 * SfH2 - Ma2 * SfH1) - Ga * SfE0);
+          part[1] = fmaf(-3.f, fmaf(sp, py, aw1), gE1 * SfG + (gB2 * SfM0 - gB0 * SfM2) +
+                                                      (Ma2 * SfH0 - Ma0 * SfH2) - Ga * SfE1);
+          part[2] = fmaf(-3.f, fmaf(sp, pz, aw2), gE2 * SfG + (gB0 * SfM1 - gB1 * SfM0) +
+                                                      (Ma0 * SfH1 - Ma1 * SfH0) - Ga * SfE2);
           part[3] = aG;
           part[4] = aM0;
           part[5] = aM1;
