@@ -38,6 +38,10 @@ constexpr int kP2PTile = 128;
 
 // Two target particles per lane group share every staged source record.
 constexpr int kTT = 2;
+// Staged source tiles whose FP32 partial sums the mixed kernel adds up before folding
+// them into its FP64 sums (every tile: 61.6 ms at N = 2^24; every 8th: 57.0 ms, error
+// vs FP64 2.12e-7 -> 2.23e-7).
+constexpr int kP2PFold = 8;
 
 
 // Number of staged tiles of target leaf c's source list (block-wide).
@@ -269,6 +273,11 @@ __global__ void __launch_bounds__(128) p2p_x2_kernel(const int *__restrict__ lea
         issue(it & 1);
       }
     }
+    // FP32 partial sums over kP2PFold tiles, then added into the FP64 sums
+    const float2 z = make_float2(0.f, 0.f);
+    float2 e0[TP], e1[TP], e2[TP], bp0[TP], bp1[TP], bp2[TP], bm0[TP], bm1[TP], bm2[TP];
+#pragma unroll
+    for (int t = 0; t < TP; ++t) e0[t] = e1[t] = e2[t] = bp0[t] = bp1[t] = bp2[t] = bm0[t] = bm1[t] = bm2[t] = z;
     for (int i = 0; i < W; ++i, ++it) {
       const int bb = it & 1;
       if (tid == 0 && i + 1 < W) {
@@ -293,10 +302,6 @@ __global__ void __launch_bounds__(128) p2p_x2_kernel(const int *__restrict__ lea
           zl[t] = make_float2((float)(dz0 - (double)zh[t].x), (float)(dz1 - (double)zh[t].y));
         }
         const float2 eps = dup2((float)kEps64);
-        const float2 z = make_float2(0.f, 0.f);
-        float2 e0[TP], e1[TP], e2[TP], bp0[TP], bp1[TP], bp2[TP], bm0[TP], bm1[TP], bm2[TP];
-#pragma unroll
-        for (int t = 0; t < TP; ++t) e0[t] = e1[t] = e2[t] = bp0[t] = bp1[t] = bp2[t] = bm0[t] = bm1[t] = bm2[t] = z;
         const float4 *S = &buf[bb][0];
         auto sweep = [&](auto NEARC) {
           constexpr bool NEAR = decltype(NEARC)::value;
@@ -341,6 +346,8 @@ __global__ void __launch_bounds__(128) p2p_x2_kernel(const int *__restrict__ lea
           sweep(std::integral_constant<bool, true>{});
         else
           sweep(std::integral_constant<bool, false>{});
+      }
+      if ((i + 1) % kP2PFold == 0 || i + 1 == W) {
 #pragma unroll
         for (int t = 0; t < TP; ++t) {
           const float2 part[6] = {e0[t], e1[t], e2[t], sub2(bp0[t], bm0[t]), sub2(bp1[t], bm1[t]),
@@ -350,6 +357,7 @@ __global__ void __launch_bounds__(128) p2p_x2_kernel(const int *__restrict__ lea
             s_acc[12 * t + q][tid] += (double)part[q].x;
             s_acc[12 * t + 6 + q][tid] += (double)part[q].y;
           }
+          e0[t] = e1[t] = e2[t] = bp0[t] = bp1[t] = bp2[t] = bm0[t] = bm1[t] = bm2[t] = z;
         }
       }
       __syncthreads();  // buffer bb is refilled two iterations later
@@ -397,13 +405,14 @@ int launch_p2p_fp64(Ctx *ctx, const int *d_leaf_ids, int64_t nleaf, bool accumul
   return ctx->check_launch("p2p_kernel");
 }
 
-// Leaves above 128 particles (G = 1): two target pairs per lane group over two lanes, which
-// halves the shared loads per evaluation (beamlets, N0 = 200: 44.1 -> 37.4 ms at 2^22); for
-// smaller leaves one pair per group keeps the register count at 80 and is faster.
+// Leaves above 64 particles (G <= 2): two target pairs per lane group over 2 G lanes, which
+// halves the shared loads per evaluation (beamlets, N0 = 200, leaves of 128: 44.1 -> 37.4 ms
+// at 2^22); for smaller leaves one pair per group keeps the register count at 80 and is faster
+// (Gaussian bunch, leaves of 64: 16.9 vs 18.0 ms).
 template <int G>
 int launch_p2p_mixed(Ctx *ctx, const int *d_leaf_ids, int64_t nleaf, bool accumulate) {
   if (nleaf <= 0) return FMMB200_OK;
-  constexpr int TP = G == 1 ? 2 : 1;
+  constexpr int TP = G <= 2 ? 2 : 1;
   constexpr int GG = G * TP;
   p2p_x2_kernel<GG, TP><<<(unsigned)nleaf, 128, 0, ctx->stream>>>(
       d_leaf_ids, (int)ctx->leaf0, ctx->get<int>("lohi"), ctx->get<int>("p2p_ptr"), ctx->get<int>("p2p_src"),
