@@ -948,6 +948,7 @@ __global__ void __launch_bounds__(MBShape1F<NDEG>::BT, MBShape1F<NDEG>::MINB)
   __shared__ double s_sn[3 * M];  // source node offsets from the own centre
   __shared__ double s_red[32 * 6];
   __shared__ double s_ct[M];
+  __shared__ int s_dir[2];  // per staged source: the boxes nearly touch (factored_ok fails)
 
   const int tid = threadIdx.x;
   const int t = blockIdx.x;
@@ -980,6 +981,8 @@ __global__ void __launch_bounds__(MBShape1F<NDEG>::BT, MBShape1F<NDEG>::MINB)
     auto issue = [&](int k, int bb) {
       const int s = src[p0 + k];
       unsigned char *dst = smem + bb * REC;
+      // written before the arrive, whose release orders it for the waiting threads
+      s_dir[bb] = !factored_ok(bbox + 6 * (int64_t)s, tb, cx, cy, cz);
       mbar_arrive_expect_tx(&bar[bb], REC);
       bulk_g2s(dst, rec32 + (int64_t)s * RECF, RAWB, &bar[bb]);
       bulk_g2s(dst + RAWB, nodes + (int64_t)s * NS, NS * 8, &bar[bb]);
@@ -1032,7 +1035,7 @@ __global__ void __launch_bounds__(MBShape1F<NDEG>::BT, MBShape1F<NDEG>::MINB)
           }
         }
         float part[NF];
-        if (!factored_ok<M>(SN, tb, cx, cy, cz)) {
+        if (s_dir[bb]) {
           // Boxes that nearly touch: the factored form of the moment adjoints, x_a . SfE - Sfe
           // and x_a x SfH - Sfh, would cancel, so those two sums are accumulated directly
           // (f R.gE_b, f R x gB_b); the other sums have no position difference and stay

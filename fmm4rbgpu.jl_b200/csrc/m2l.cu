@@ -247,6 +247,7 @@ __global__ void __launch_bounds__(M2LShape2<NDEG>::BT)
   double *s_acc = (double *)(smem + 2 * REC + 5 * NN * 16);
   __shared__ __align__(8) uint64_t bar[2];
   __shared__ double s_sn[3 * M];  // source node offsets from the target centre
+  __shared__ int s_dir[2];        // per staged source: direct sums (the boxes nearly touch)
 
   const int tid = threadIdx.x;
   const int t = blockIdx.x;
@@ -272,6 +273,10 @@ __global__ void __launch_bounds__(M2LShape2<NDEG>::BT)
     auto issue = [&](int k, int bb) {
       const int s = src[p0 + k];
       unsigned char *dst = smem + bb * REC;
+      // factored sums unless the two boxes nearly touch (factored_ok); at N = 2^24 the
+      // direct pairs make the M2L about 2 % slower and its error ~20x smaller.  Written
+      // before the arrive, whose release orders it for the threads that wait on bar[bb].
+      s_dir[bb] = MASK || !factored_ok(bbox + 6 * (int64_t)s, tb, cx, cy, cz);
       mbar_arrive_expect_tx(&bar[bb], REC);
       bulk_g2s(dst, mom + (int64_t)s * 4 * NN, MOM_BYTES, &bar[bb]);
       bulk_g2s(dst + MOM_BYTES, nodes + (int64_t)s * NS, NS * 8, &bar[bb]);
@@ -288,9 +293,7 @@ __global__ void __launch_bounds__(M2LShape2<NDEG>::BT)
       const bool ok = mbar_wait_bounded(&bar[bb], (uint32_t)((i >> 1) & 1), status);
       const float *G = (const float *)(smem + bb * REC);
       const double *SN = (const double *)(smem + bb * REC + MOM_BYTES);
-      // factored sums unless the two boxes nearly touch (factored_ok); at N = 2^24 the
-      // direct pairs make the M2L about 4 % slower and its error ~20x smaller
-      const bool dir = MASK || !factored_ok<M>(SN, tb, cx, cy, cz);
+      const bool dir = s_dir[bb] != 0;
       if (ok) {
         for (int e = tid; e < 3 * M; e += BT) {
           const int d = e / M;
@@ -764,7 +767,7 @@ __global__ void m2l_split_count_kernel(int64_t nc, const int *__restrict__ ptr, 
     const double *tb = bbox + 6 * t;
     const double cx = 0.5 * (tb[0] + tb[3]), cy = 0.5 * (tb[1] + tb[4]), cz = 0.5 * (tb[2] + tb[5]);
     for (int k = ptr[t]; k < ptr[t + 1]; ++k) {
-      if (factored_ok<M>(nodes + (int64_t)src[k] * NS, tb, cx, cy, cz))
+      if (factored_ok(bbox + 6 * (int64_t)src[k], tb, cx, cy, cz))
         ++a;
       else
         ++b;
@@ -786,7 +789,7 @@ __global__ void m2l_split_write_kernel(int64_t nc, const int *__restrict__ ptr, 
   int oa = ptr2[t], ob = ptr2[nc + 1 + t];
   for (int k = ptr[t]; k < ptr[t + 1]; ++k) {
     const int s = src[k];
-    if (factored_ok<M>(nodes + (int64_t)s * NS, tb, cx, cy, cz))
+    if (factored_ok(bbox + 6 * (int64_t)s, tb, cx, cy, cz))
       src_a[oa++] = s;
     else
       src_b[ob++] = s;

@@ -40,19 +40,17 @@ __device__ __forceinline__ void kahan_add2(float2 &sum, float2 &comp, float2 v) 
 // The FP32 M2L kernels factor their sums over the source nodes y_b around the target
 // centre (E = x' G - Q and the like), which loses a factor (|x'| + |y|) / |x' - y| of
 // precision for a target node x' and a source node y.  True when that factor stays
-// below kFactoredMaxCancel for every node pair of the target box (centre c, lower
-// corner tb[0..2], upper tb[3..5]) and the source box spanned by its M Chebyshev nodes
-// per axis (sn[d M + i]): |x'| <= |h_t|, |y| <= |c_s - c| + |h_s|, and |x' - y| is at
-// least the distance between the boxes.  Pairs of boxes that nearly touch fail it.
+// below kFactoredMaxCancel for every node pair of the target box (centre c, corners
+// tb[0..2], tb[3..5]) and the source box (corners sb[0..2], sb[3..5]): |x'| <= |h_t|,
+// |y| <= |c_s - c| + |h_s|, and |x' - y| is at least the distance between the boxes.
+// Pairs of boxes that nearly touch fail it.
 constexpr double kFactoredMaxCancel = 16.0;
 
-template <int M>
-__device__ __forceinline__ bool factored_ok(const double *sn, const double *tb, double cx, double cy, double cz) {
+__device__ __forceinline__ bool factored_ok(const double *sb, const double *tb, double cx, double cy, double cz) {
   double R2 = 0.0, gap2 = 0.0, rt2 = 0.0, rs2 = 0.0;
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
-    const double a = sn[d * M + M - 1], b = sn[d * M];
-    const double lo = fmin(a, b), hi = fmax(a, b);
+    const double lo = sb[d], hi = sb[3 + d];
     const double hs = 0.5 * (hi - lo), ht = 0.5 * (tb[3 + d] - tb[d]);
     const double dc = fabs(0.5 * (lo + hi) - (d == 0 ? cx : (d == 1 ? cy : cz)));
     const double g = fmax(0.0, dc - hs - ht);
