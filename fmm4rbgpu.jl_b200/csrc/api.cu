@@ -585,10 +585,11 @@ int fmmb200_forward(fmmb200_ctx *ctx, int64_t npar, const double *pos, const dou
   FMM_TRY(ctx->ensure("out_e", 3 * npar, &de));
   FMM_TRY(ctx->ensure("out_b", 3 * npar, &db));
   mark(ctx, kEvStart);
-  // positions on the stream; momenta on the copy stream, overlapping the position-only
-  // start of the tree build (finite check, radix sorts)
-  FMM_CUDA_TRY(ctx, cudaEventRecord(ctx->ev_copy[0], ctx->stream));
+  // positions on the stream; momenta on the copy stream once the positions are in (the two
+  // copies would otherwise share the link and delay the positions), overlapping the
+  // position-only start of the tree build (finite check, radix sorts)
   FMM_CUDA_TRY(ctx, cudaMemcpyAsync(dp, pos, sizeof(double) * 3 * npar, cudaMemcpyHostToDevice, ctx->stream));
+  FMM_CUDA_TRY(ctx, cudaEventRecord(ctx->ev_copy[0], ctx->stream));
   FMM_CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->copy_stream, ctx->ev_copy[0], 0));
   FMM_CUDA_TRY(ctx, cudaMemcpyAsync(dm, mom, sizeof(double) * 3 * npar, cudaMemcpyHostToDevice, ctx->copy_stream));
   FMM_CUDA_TRY(ctx, cudaEventRecord(ctx->ev_copy[1], ctx->copy_stream));

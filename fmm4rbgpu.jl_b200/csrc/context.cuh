@@ -13,7 +13,7 @@ struct fmmb200_ctx {
   cudaStream_t own_stream = nullptr;
   cudaStream_t stream = nullptr;
   // the host-pointer forward copies the momenta here while the stream starts the tree
-  // build on the positions; ev_copy[0]: inputs free to overwrite, [1]: momenta copied
+  // build on the positions; ev_copy[0]: positions copied, [1]: momenta copied
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t ev_copy[2] = {};
   std::string err;
