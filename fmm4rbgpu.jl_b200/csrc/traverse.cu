@@ -9,6 +9,7 @@
 // outputs at offsets from a block scan, so every step is deterministic.  The
 // set of emitted pairs equals the DFS's.  Both lists are then radix-sorted by
 // (target, source) and grouped into CSR pointers over all clusters.
+#include <algorithm>
 #include <string>
 
 #include "device_util.cuh"
@@ -218,7 +219,11 @@ int grow_keep(Ctx *ctx, const char *name, size_t used, size_t need, void **out) 
 int sort_and_group(Ctx *ctx, const char *keys_name, const char *alt_name, const char *ptr_name,
                    const char *src_name, int64_t n, int bits) {
   uint64_t *keys = ctx->get<uint64_t>(keys_name), *alt = nullptr;
-  FMM_TRY(ctx->ensure(alt_name, n, &alt));
+  // The sort may end in the alternate buffer, and then the two names swap.  Giving the
+  // alternate the keys buffer's capacity keeps the traversal's next call from finding a
+  // smaller buffer under keys_name and reallocating it (a synchronising free and copy).
+  const int64_t kcap = (int64_t)(ctx->bufs[keys_name].cap / sizeof(uint64_t));
+  FMM_TRY(ctx->ensure(alt_name, std::max(n, kcap), &alt));
   keys = ctx->get<uint64_t>(keys_name);
   bool in_alt = false;
   FMM_TRY(radix_sort(ctx, keys, alt, nullptr, nullptr, n, 2 * bits, &in_alt));
