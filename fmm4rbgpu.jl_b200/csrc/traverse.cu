@@ -9,7 +9,6 @@
 // outputs at offsets from a block scan, so every step is deterministic.  The
 // set of emitted pairs equals the DFS's.  Both lists are then radix-sorted by
 // (target, source) and grouped into CSR pointers over all clusters.
-#include <algorithm>
 #include <string>
 
 #include "device_util.cuh"
@@ -219,16 +218,14 @@ int grow_keep(Ctx *ctx, const char *name, size_t used, size_t need, void **out) 
 int sort_and_group(Ctx *ctx, const char *keys_name, const char *alt_name, const char *ptr_name,
                    const char *src_name, int64_t n, int bits) {
   uint64_t *keys = ctx->get<uint64_t>(keys_name), *alt = nullptr;
-  // The sort may end in the alternate buffer, and then the two names swap.  Giving the
-  // alternate the keys buffer's capacity keeps the traversal's next call from finding a
-  // smaller buffer under keys_name and reallocating it (a synchronising free and copy).
-  const int64_t kcap = (int64_t)(ctx->bufs[keys_name].cap / sizeof(uint64_t));
-  FMM_TRY(ctx->ensure(alt_name, std::max(n, kcap), &alt));
+  FMM_TRY(ctx->ensure(alt_name, n, &alt));
   keys = ctx->get<uint64_t>(keys_name);
   bool in_alt = false;
   FMM_TRY(radix_sort(ctx, keys, alt, nullptr, nullptr, n, 2 * bits, &in_alt));
-  if (in_alt) std::swap(ctx->bufs[keys_name], ctx->bufs[alt_name]);
-  keys = ctx->get<uint64_t>(keys_name);
+  // Copied back rather than swapping the two names: the keys buffer keeps the traversal's
+  // capacity, so the next traversal does not reallocate it (a synchronising free and copy).
+  if (in_alt && n > 0)
+    FMM_CUDA_TRY(ctx, cudaMemcpyAsync(keys, alt, sizeof(uint64_t) * n, cudaMemcpyDeviceToDevice, ctx->stream));
   int *ptr, *src;
   FMM_TRY(ctx->ensure(ptr_name, ctx->nc + 1, &ptr));
   FMM_TRY(ctx->ensure(src_name, n, &src));
