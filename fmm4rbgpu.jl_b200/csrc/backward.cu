@@ -1399,8 +1399,12 @@ __global__ void adj_p2p_rec_kernel(int N, const float4 *__restrict__ prec32x2, c
 // parts as in the mixed forward.  The particle itself is skipped, as in the FP64
 // adjoint; a distinct particle at the same position keeps the regularised
 // kernel's finite derivative (f = eps^-3/2 times c; the f5 term is formed as
-// f (s^2 (R.c)) and vanishes without overflowing).  Per tile the FP32 partial sums
-// are added into FP64 sums in shared memory.
+// f (s^2 (R.c)) and vanishes without overflowing).  The FP32 partial sums of
+// kPbFold tiles at a time are added into FP64 sums in shared memory.  Tiles whose
+// boxes are apart by more than 1/16 of the larger extent form R from the hi parts
+// alone, as in the forward.
+constexpr int kPbFold = 8;
+
 template <int G>
 __global__ void __launch_bounds__(128)
     p2p_bwd_x2_kernel(int leaf0, const int *__restrict__ lohi, const int *__restrict__ ptr,
@@ -1410,12 +1414,13 @@ __global__ void __launch_bounds__(128)
   constexpr int REC = 9;  // float4 per source record (the last one padding)
   __shared__ __align__(16) float4 buf[2][kPbTile * REC];
   __shared__ __align__(8) uint64_t bar[2];
-  __shared__ int s_cnt[2], s_flag[2], s_first[2];
+  __shared__ int s_cnt[2], s_flag[2], s_first[2], s_near[2];
   __shared__ double s_centre[2][3];
   __shared__ int s_warp[33];
   __shared__ double s_acc[14][128];  // per thread: gx(3), gu(3), sw of both targets, FP64
   const int tid = threadIdx.x, TG = blockDim.x / G, tl = tid / G, g = tid % G;
   const int c = leaf0 + blockIdx.x;
+  const double *tbox = bbox + 6 * (int64_t)c;
   const int tlo = lohi[2 * c], thi = lohi[2 * c + 1], tcnt = thi - tlo + 1;
   const int p0 = ptr[c], np = ptr[c + 1] - p0;
   int w = 0;
@@ -1443,6 +1448,12 @@ __global__ void __launch_bounds__(128)
     s_centre[bb][0] = 0.5 * (sb[0] + sb[3]);
     s_centre[bb][1] = 0.5 * (sb[1] + sb[4]);
     s_centre[bb][2] = 0.5 * (sb[2] + sb[5]);
+    double gap = 0.0, ext = 0.0;
+    for (int d = 0; d < 3; ++d) {
+      gap = fmax(gap, fmax(sb[d] - tbox[3 + d], tbox[d] - sb[3 + d]));
+      ext = fmax(ext, fmax(sb[3 + d] - sb[d], tbox[3 + d] - tbox[d]));
+    }
+    s_near[bb] = !(16.0 * gap > ext);
     const uint32_t bytes = (uint32_t)(cnt * REC * sizeof(float4));
     mbar_arrive_expect_tx(&bar[bb], bytes);
     bulk_g2s(&buf[bb][0], recb + (int64_t)(slo + woff) * REC, bytes, &bar[bb]);
@@ -1477,6 +1488,7 @@ __global__ void __launch_bounds__(128)
         issue(it & 1);
       }
     }
+    float2 gx0 = z, gx1 = z, gx2 = z, gu0 = z, gu1 = z, gu2 = z, sw = z, ser = z;
     for (int i = 0; i < W; ++i, ++it) {
       const int bb = it & 1;
       if (tid == 0 && i + 1 < W) {
@@ -1496,17 +1508,25 @@ __global__ void __launch_bounds__(128)
         const float2 xl = make_float2((float)(dx0 - (double)xh.x), (float)(dx1 - (double)xh.y));
         const float2 yl = make_float2((float)(dy0 - (double)yh.x), (float)(dy1 - (double)yh.y));
         const float2 zl = make_float2((float)(dz0 - (double)zh.x), (float)(dz1 - (double)zh.y));
-        float2 gx0 = z, gx1 = z, gx2 = z, gu0 = z, gu1 = z, gu2 = z, sw = z, ser = z;
         const float4 *S = &buf[bb][0];
-        auto sweep = [&](auto FL) {
+        auto sweep = [&](auto FL, auto NEARC) {
           constexpr int F = decltype(FL)::value;
+          constexpr bool NEAR = decltype(NEARC)::value;
 #pragma unroll 2
           for (int j = g; j < cnt; j += G) {
             const float4 *q = S + j * REC;
-            const float4 q0 = q[0], q1 = q[1], q2 = q[2];
-            const float2 rx = add2(add2(xh, lo2(q0)), add2(xl, hi2(q1)));
-            const float2 ry = add2(add2(yh, hi2(q0)), add2(yl, lo2(q2)));
-            const float2 rz = add2(add2(zh, lo2(q1)), add2(zl, hi2(q2)));
+            const float4 q0 = q[0], q1 = q[1];
+            float2 rx, ry, rz;
+            if constexpr (NEAR) {
+              const float4 q2 = q[2];
+              rx = add2(add2(xh, lo2(q0)), add2(xl, hi2(q1)));
+              ry = add2(add2(yh, hi2(q0)), add2(yl, lo2(q2)));
+              rz = add2(add2(zh, lo2(q1)), add2(zl, hi2(q2)));
+            } else {
+              rx = add2(xh, lo2(q0));
+              ry = add2(yh, hi2(q0));
+              rz = add2(zh, lo2(q1));
+            }
             const float2 rr = fma2(rx, rx, fma2(ry, ry, mul2(rz, rz)));
             if constexpr ((F & 1) != 0) {  // j's field at the target: uses u_j, gamma_j and the target's a_E, a_B
               const float4 q3 = q[3], q4 = q[4];
@@ -1554,12 +1574,25 @@ __global__ void __launch_bounds__(128)
             }
           }
         };
-        if (fl == 3)
-          sweep(std::integral_constant<int, 3>{});
-        else if (fl == 1)
-          sweep(std::integral_constant<int, 1>{});
-        else if (fl == 2)
-          sweep(std::integral_constant<int, 2>{});
+        const std::true_type near_tile{};
+        const std::false_type far_tile{};
+        if (s_near[bb]) {
+          if (fl == 3)
+            sweep(std::integral_constant<int, 3>{}, near_tile);
+          else if (fl == 1)
+            sweep(std::integral_constant<int, 1>{}, near_tile);
+          else if (fl == 2)
+            sweep(std::integral_constant<int, 2>{}, near_tile);
+        } else {
+          if (fl == 3)
+            sweep(std::integral_constant<int, 3>{}, far_tile);
+          else if (fl == 1)
+            sweep(std::integral_constant<int, 1>{}, far_tile);
+          else if (fl == 2)
+            sweep(std::integral_constant<int, 2>{}, far_tile);
+        }
+      }
+      if ((i + 1) % kPbFold == 0 || i + 1 == W) {
         const float2 sg = mul2(ser, igp);
         const float2 part[7] = {gx0, gx1, gx2, fma2(sg, up0, gu0), fma2(sg, up1, gu1), fma2(sg, up2, gu2), sw};
 #pragma unroll
@@ -1567,6 +1600,7 @@ __global__ void __launch_bounds__(128)
           s_acc[q][tid] += (double)part[q].x;
           s_acc[7 + q][tid] += (double)part[q].y;
         }
+        gx0 = gx1 = gx2 = gu0 = gu1 = gu2 = sw = ser = z;
       }
       __syncthreads();  // buffer bb is refilled two iterations later
     }

@@ -289,8 +289,9 @@ int build_lists(Ctx *ctx, double eta, const double *d_consts) {
   int64_t cap_p = 64 * ctx->nleaf + 1024, cap_m = 32 * nc + 1024;
   int2 *fa, *fb;
   uint64_t *p2p, *m2l;
-  FMM_TRY(ctx->ensure("front_a", 4 * nc + 1024, &fa));
-  FMM_TRY(ctx->ensure("front_b", 4 * nc + 1024, &fb));
+  int64_t front_need = 4 * nc + 1024;  // elements, the largest frontier buffer this traversal asks for
+  FMM_TRY(ctx->ensure("front_a", front_need, &fa));
+  FMM_TRY(ctx->ensure("front_b", front_need, &fb));
   void *vp;
   FMM_TRY(grow_keep(ctx, "p2p_keys", 0, sizeof(uint64_t) * cap_p, &vp));
   FMM_TRY(grow_keep(ctx, "m2l_keys", 0, sizeof(uint64_t) * cap_m, &vp));
@@ -319,6 +320,7 @@ int build_lists(Ctx *ctx, double eta, const double *d_consts) {
     FMM_TRY(grow_keep(ctx, "m2l_keys", sizeof(uint64_t) * nm2l, sizeof(uint64_t) * (nm2l + tm), &vp));
     m2l = (uint64_t *)vp;
     FMM_TRY(ctx->ensure("front_b", 2 * ts + 1, &fb));  // destination: contents not needed
+    if (2 * ts + 1 > front_need) front_need = 2 * ts + 1;
     trav_write_kernel<<<nblk, kTvThreads, 0, ctx->stream>>>(fa, (int)nf, geom, d_consts, eta, nblk, boff, bits,
                                                              p2p + np2p, m2l + nm2l, fb);
     FMM_TRY(ctx->check_launch("trav_write_kernel"));
@@ -331,6 +333,12 @@ int build_lists(Ctx *ctx, double eta, const double *d_consts) {
     ++steps;
     if (steps > 4 * 64) return ctx->fail(FMMB200_ERR_DEVICE, "traversal did not terminate");
   }
+  // The two frontier buffers swap every step, so a step may grow either one.  Sizing both for
+  // the largest frontier of this traversal here (neither holds live data now) means the next
+  // traversal of the same tree grows neither.  The request is a need, never a capacity, so
+  // repeated calls cannot compound the allocator's headroom.
+  FMM_TRY(ctx->ensure("front_a", front_need, &fa));
+  FMM_TRY(ctx->ensure("front_b", front_need, &fb));
   ctx->nm2l = nm2l;
   ctx->np2p = np2p;
   ctx->traversal_steps = steps;

@@ -193,6 +193,22 @@ def test_deterministic(gpu_ctx):
     assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_device_memory_is_steady_across_calls(gpu_ctx, precision):
+    """Repeated forwards of one beam allocate nothing after the first: the library's device
+    memory is the same after every call (a fresh context, so the first call sizes it)."""
+    import fmmb200
+
+    pos, mom = make("gauss", 60000, 5)
+    alg = fmmb200.FMMB200(n=4, N0=64, eta=0.5, precision=precision)
+    with fmmb200.Context(0) as ctx:
+        sizes = []
+        for _ in range(6):
+            ctx.forward(pos, mom, alg)
+            sizes.append(ctx.stats()["device_bytes"])
+    assert len(set(sizes)) == 1, sizes
+
+
 @pytest.mark.parametrize("N,N0", [(1, 125), (2, 125), (100, 200), (125, 125)])
 def test_single_leaf_equals_direct_sum(gpu_ctx, oracle_mod, N, N0):
     import fmmb200
