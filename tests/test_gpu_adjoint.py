@@ -103,6 +103,14 @@ def test_gradient_matches_finite_differences(gpu_ctx, n, N0):
     assert rel(an, fd) < 1e-4, (rel(an, fd), np.c_[fd, an][:8])
 
 
+def test_gradient_matches_finite_differences_at_262144(gpu_ctx):
+    """The same check on a 262,144-particle Gaussian bunch, n = 4, N0 = 125, eta = 1/2."""
+    import fmmb200
+
+    fd, an = _fd_case(gpu_ctx, fmmb200.FMMB200(n=4, N0=125, eta=0.5), 262144)
+    assert rel(an, fd) < 1e-4, rel(an, fd)
+
+
 def test_mixed_forward_adjoint_matches_fp64(gpu_ctx):
     import fmmb200
     from fmmb200 import beams
