@@ -69,6 +69,9 @@ struct fmmb200_ctx {
   }
 
   // Device buffer `name` with at least `bytes` bytes (contents not preserved on growth).
+  // Buffer `name` of at least `bytes`, reallocated (contents lost) only when smaller.  A new
+  // allocation gets 1/8 headroom, so `bytes` must be a need: a request derived from another
+  // buffer's capacity would grow by that headroom on every call.
   int ensure_bytes(const char *name, size_t bytes, void **out) {
     Buf &b = bufs[name];
     if (bytes == 0) bytes = 16;
