@@ -32,21 +32,29 @@ std::mutex g_noalloc_mutex;
 constexpr int kDirThreads = 128;
 constexpr int kDirTile = 256;
 
+// A target index outside [0, N) is never dereferenced: that target's partials are
+// NaN, and `status` (when given) is raised to kDevBadIndex.
 __global__ void __launch_bounds__(kDirThreads)
     direct_partial_kernel(int64_t N, const double *__restrict__ pos, const double *__restrict__ mom,
                           int64_t ntarget, const int64_t *__restrict__ targets, int splits,
-                          double *__restrict__ part) {
+                          double *__restrict__ part, int *__restrict__ status) {
   __shared__ double s[kDirTile][7];
   const int64_t q = (int64_t)blockIdx.x * kDirThreads + threadIdx.x;
   const int split = blockIdx.y;
   const int64_t per = (N + splits - 1) / splits;
   const int64_t j0 = split * per, j1 = j0 + per < N ? j0 + per : N;
   double xi = 0, yi = 0, zi = 0;
+  bool bad = false;
   if (q < ntarget) {
     const int64_t i = targets ? targets[q] : q;
-    xi = pos[3 * i];
-    yi = pos[3 * i + 1];
-    zi = pos[3 * i + 2];
+    bad = i < 0 || i >= N;
+    if (bad) {
+      if (status && split == 0) atomicCAS(status, kDevOk, kDevBadIndex);
+    } else {
+      xi = pos[3 * i];
+      yi = pos[3 * i + 1];
+      zi = pos[3 * i + 2];
+    }
   }
   double e0 = 0, e1 = 0, e2 = 0, b0 = 0, b1 = 0, b2 = 0;
   for (int64_t t0 = j0; t0 < j1; t0 += kDirTile) {
@@ -84,6 +92,7 @@ __global__ void __launch_bounds__(kDirThreads)
     }
   }
   if (q < ntarget) {
+    if (bad) e0 = e1 = e2 = b0 = b1 = b2 = __longlong_as_double(0x7ff8000000000000ll);
     double *o = part + ((int64_t)split * ntarget + q) * 6;
     o[0] = e0;
     o[1] = e1;
@@ -162,10 +171,12 @@ int run_direct(Ctx *ctx, int64_t N, const double *d_pos, const double *d_mom, do
   double *part;
   FMM_TRY(ctx->ensure("direct_part", 6 * ntarget * splits, &part));
   dim3 grid((unsigned)tblocks, (unsigned)splits);
-  direct_partial_kernel<<<grid, kDirThreads, 0, ctx->stream>>>(N, d_pos, d_mom, ntarget, d_targets, splits, part);
+  direct_partial_kernel<<<grid, kDirThreads, 0, ctx->stream>>>(N, d_pos, d_mom, ntarget, d_targets, splits, part,
+                                                               ctx->d_status);
   direct_reduce_kernel<<<ceil_div(ntarget, 256), 256, 0, ctx->stream>>>(ntarget, splits, part,
                                                                         kRe * charge / lambda, d_e, d_b);
-  return ctx->check_launch("direct kernels", 2);
+  FMM_TRY(ctx->check_launch("direct kernels", 2));
+  return ctx->check_device_status("direct");
 }
 
 }  // namespace
@@ -178,7 +189,10 @@ int fmmb200_direct_device(fmmb200_ctx *ctx, int64_t npar, const double *d_positi
   if (!ctx) return FMMB200_ERR_INVALID_ARGUMENT;
   if (npar < 1 || !d_positions || !d_momenta || !d_efields || !d_bfields || ntarget < 1)
     return ctx->fail(FMMB200_ERR_INVALID_ARGUMENT, "direct: bad arguments");
+  if (!d_targets && ntarget > npar)
+    return ctx->fail(FMMB200_ERR_INVALID_ARGUMENT, "direct: ntarget > npar without a target list");
   if (!(lambda != 0.0)) return ctx->fail(FMMB200_ERR_INVALID_ARGUMENT, "lambda must be nonzero");
+  cudaSetDevice(ctx->device);
   return run_direct(ctx, npar, d_positions, d_momenta, charge, lambda, ntarget, d_targets, d_efields, d_bfields);
 }
 
@@ -216,22 +230,20 @@ int fmmb200_direct_noalloc(int64_t npar, const double *d_positions, const double
                            double *d_bfields, void *stream) {
   if (npar < 1 || ntarget < 1 || !d_positions || !d_momenta || !d_efields || !d_bfields || !(lambda != 0.0))
     return FMMB200_ERR_INVALID_ARGUMENT;
+  if (!d_targets && ntarget > npar) return FMMB200_ERR_INVALID_ARGUMENT;
   if (ntarget > kNoAllocSlots) return FMMB200_ERR_CAPACITY;
+  // This entry point owns no error state: it reads errors with cudaPeekAtLastError and
+  // leaves a pending error of the caller's in place.
+  if (cudaPeekAtLastError() != cudaSuccess) return FMMB200_ERR_CUDA;
   int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
-    cudaGetLastError();
-    return FMMB200_ERR_CUDA;
-  }
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return FMMB200_ERR_CUDA;
   double *scratch;
   {
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
     if (!g_noalloc_ptr[dev]) {
       // once per device, with that device current: the device address of the array
       double *p = nullptr;
-      if (cudaGetSymbolAddress((void **)&p, g_noalloc_scratch) != cudaSuccess || !p) {
-        cudaGetLastError();
-        return FMMB200_ERR_CUDA;
-      }
+      if (cudaGetSymbolAddress((void **)&p, g_noalloc_scratch) != cudaSuccess || !p) return FMMB200_ERR_CUDA;
       g_noalloc_ptr[dev] = p;
     }
     scratch = g_noalloc_ptr[dev];
@@ -240,10 +252,11 @@ int fmmb200_direct_noalloc(int64_t npar, const double *d_positions, const double
   const int64_t tblocks = (ntarget + kDirThreads - 1) / kDirThreads;
   cudaStream_t st = (cudaStream_t)stream;
   dim3 grid((unsigned)tblocks, (unsigned)splits);
-  direct_partial_kernel<<<grid, kDirThreads, 0, st>>>(npar, d_positions, d_momenta, ntarget, d_targets, splits, scratch);
+  direct_partial_kernel<<<grid, kDirThreads, 0, st>>>(npar, d_positions, d_momenta, ntarget, d_targets, splits, scratch,
+                                                       nullptr);
   direct_reduce_kernel<<<ceil_div(ntarget, 256), 256, 0, st>>>(ntarget, splits, scratch, kRe * charge / lambda,
                                                                d_efields, d_bfields);
-  if (cudaGetLastError() != cudaSuccess) return FMMB200_ERR_CUDA;
+  if (cudaPeekAtLastError() != cudaSuccess) return FMMB200_ERR_CUDA;
   return FMMB200_OK;
 }
 

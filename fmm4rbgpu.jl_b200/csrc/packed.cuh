@@ -28,15 +28,6 @@ __device__ __forceinline__ float rsqrt_approx_f32(float x) {
 }
 __device__ __forceinline__ float2 rsqrt2(float2 d) { return make_float2(rsqrt_approx_f32(d.x), rsqrt_approx_f32(d.y)); }
 
-// Kahan-compensated accumulation of v into (sum, comp), lane by lane; the value
-// held is sum - comp.
-__device__ __forceinline__ void kahan_add2(float2 &sum, float2 &comp, float2 v) {
-  const float2 y = sub2(v, comp);
-  const float2 t = add2(sum, y);
-  comp = sub2(sub2(t, sum), y);
-  sum = t;
-}
-
 // The FP32 M2L kernels factor their sums over the source nodes y_b around the target
 // centre (E = x' G - Q and the like), which loses a factor (|x'| + |y|) / |x' - y| of
 // precision for a target node x' and a source node y.  True when that factor stays

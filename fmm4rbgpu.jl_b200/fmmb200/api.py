@@ -78,7 +78,8 @@ class FMMB200:
     """The B200 algorithm selector; fields as the reference's FMMGPU (n, N0, eta).
 
     ``precision`` is "fp64" (the plain FP64 path, the drop-in) or "mixed" (FP32
-    arithmetic with compensated sums, FP64 geometry and final accumulation).
+    arithmetic whose per-source partial sums are folded into FP64 sums, FP64
+    geometry and final accumulation).
     """
 
     n: int

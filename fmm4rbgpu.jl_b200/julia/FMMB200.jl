@@ -5,29 +5,32 @@
 # the library's hand-written adjoint.
 #
 # Usage (next to `using FMM4RBGPU`):
-#     include("FMMB200.jl"); using .FMMB200
+#     include("FMMB200.jl"); using .FMMB200Binding
 #     update_particles_field!(beam, FMMB200(0.5, 125, 4); lambda=1.0)
 #     update_particles_field!(beam, FMMB200(0.5, 125, 4; precision=:mixed); lambda=1.0)
+#     update_particles_field!(beam, FMMB200(eta=0.5, N0=125, n=4); lambda=1.0)
+#
+# The module is called FMMB200Binding so that the name FMMB200 is free for the
+# algorithm constructor (a module binds its own name inside itself).
 #
 # Every call is synchronous; a nonzero status from the library is raised as an
 # ErrorException carrying fmmb200_last_error (the reference's error behaviour).
-module FMMB200
+module FMMB200Binding
 
 using FMM4RBGPU: Particles
 import FMM4RBGPU: update_particles_field!
 using ChainRulesCore
 
-export FMMB200Alg, fmm_fields
+export FMMB200, FMMB200Alg, fmm_fields, update_particles_field!
 
 const libfmmb200 = get(ENV, "FMMB200_LIB", joinpath(@__DIR__, "..", "lib", "libfmmb200.so"))
 
 """
-    FMMB200Alg(; n, N0, eta, precision=:fp64)
-    FMMB200Alg(eta, N0, n; precision=:fp64)
+    FMMB200Alg{T}(n, N0, eta, precision)
 
 The B200 FMM: interpolation degree `n` (1..10), leaf size `N0`, admissibility
 `eta` -- the fields of `FMMGPU` (src/update_particles_field.jl:15-19) --
-and `precision` `:fp64` (the plain path) or `:mixed`.
+and `precision` `:fp64` (the plain path) or `:mixed`.  Build it with `FMMB200`.
 """
 Base.@kwdef struct FMMB200Alg{T}
     n::Int
@@ -35,9 +38,17 @@ Base.@kwdef struct FMMB200Alg{T}
     eta::T
     precision::Symbol = :fp64
 end
-FMMB200Alg(eta::Real, N0::Integer, n::Integer; precision::Symbol=:fp64) =
+
+"""
+    FMMB200(eta, N0, n; precision=:fp64)
+    FMMB200(; n, N0, eta, precision=:fp64)
+
+The algorithm selector of the field-evaluation call, in the positional order
+`(eta, N0, n)` or by keyword like `FMMGPU(eta=..., N0=..., n=...)` (README.md:55).
+"""
+FMMB200(eta::Real, N0::Integer, n::Integer; precision::Symbol=:fp64) =
     FMMB200Alg(n=Int(n), N0=Int(N0), eta=eta, precision=precision)
-const FMMB200 = FMMB200Alg   # the spelling of the field-evaluation call: FMMB200(eta, N0, n)
+FMMB200(; n::Integer, N0::Integer, eta::Real, precision::Symbol=:fp64) = FMMB200(eta, N0, n; precision=precision)
 
 _prec(alg) = alg.precision === :mixed ? Int32(1) : alg.precision === :fp64 ? Int32(0) :
     throw(ArgumentError("precision must be :fp64 or :mixed"))
@@ -58,14 +69,34 @@ mutable struct Context
     end
 end
 
+_error(ctx::Context, st::Cint) = ErrorException(
+    "libfmmb200 status $st: " * unsafe_string(ccall((:fmmb200_last_error, libfmmb200), Cstring, (Ptr{Cvoid},), ctx.ptr)))
+
 function _check(ctx::Context, st::Cint)
-    st == 0 && return nothing
-    msg = unsafe_string(ccall((:fmmb200_last_error, libfmmb200), Cstring, (Ptr{Cvoid},), ctx.ptr))
-    throw(ErrorException("libfmmb200 status $st: $msg"))
+    st == 0 || throw(_error(ctx, st))
+    return nothing
 end
 
 const _DEFAULT = Ref{Union{Nothing,Context}}(nothing)
-default_context() = something(_DEFAULT[], (_DEFAULT[] = Context(0)))
+const _DEFAULT_LOCK = ReentrantLock()
+default_context() = lock(_DEFAULT_LOCK) do
+    something(_DEFAULT[], (_DEFAULT[] = Context(0)))
+end
+
+# Contexts that hold a forward saved for a pullback.  A context holds one saved
+# forward at a time, so each differentiated call takes one from this pool (making
+# one only when the pool is empty) and its pullback puts it back after the
+# adjoint has run; a loop of forward + pullback reuses the same context and its
+# device buffers.  A context whose pullback never runs is freed by its finalizer.
+const _POOL = Context[]
+const _POOL_LOCK = ReentrantLock()
+_acquire() = lock(_POOL_LOCK) do
+    isempty(_POOL) ? Context(0) : pop!(_POOL)
+end
+_release(ctx::Context) = lock(_POOL_LOCK) do
+    push!(_POOL, ctx)
+    nothing
+end
 
 """
     update_particles_field!(particles::Particles{Float64}, alg::FMMB200Alg; lambda)
@@ -113,9 +144,16 @@ fmm_fields(pos::Matrix{Float64}, mom::Matrix{Float64}, alg::FMMB200Alg; charge=-
 
 function ChainRulesCore.rrule(::typeof(fmm_fields), pos::Matrix{Float64}, mom::Matrix{Float64},
                               alg::FMMB200Alg; charge=-1.0, lambda=1.0)
-    ctx = Context(0)  # the saved forward lives in this context until the pullback runs
-    E, B = _forward!(ctx, pos, mom, alg, charge, lambda, true)
+    ctx = _acquire()  # the saved forward lives in this context until the pullback runs
+    E, B = try
+        _forward!(ctx, pos, mom, alg, charge, lambda, true)
+    catch
+        _release(ctx)
+        rethrow()
+    end
+    released = Ref(false)
     function fmm_fields_pullback(Δ)
+        released[] && error("fmm_fields pullback called twice: the saved forward is gone")
         ΔE, ΔB = unthunk(Δ[1]), unthunk(Δ[2])
         gE = ΔE isa AbstractZero ? zeros(size(pos)) : Matrix{Float64}(ΔE)
         gB = ΔB isa AbstractZero ? zeros(size(pos)) : Matrix{Float64}(ΔB)
@@ -123,7 +161,10 @@ function ChainRulesCore.rrule(::typeof(fmm_fields), pos::Matrix{Float64}, mom::M
         gu = similar(pos)
         st = ccall((:fmmb200_backward, libfmmb200), Cint,
                    (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}), ctx.ptr, gE, gB, gx, gu)
-        _check(ctx, st)
+        err = st == 0 ? nothing : _error(ctx, st)  # read before another call can take ctx
+        released[] = true
+        _release(ctx)
+        err === nothing || throw(err)
         return NoTangent(), gx, gu, NoTangent()
     end
     return (E, B), fmm_fields_pullback

@@ -46,7 +46,7 @@ extern "C" {
 #define FMMB200_ERR_CAPACITY 7     /* larger than a fixed-size scratch array allows */
 
 #define FMMB200_PRECISION_FP64 0   /* plain FP64 path (the drop-in) */
-#define FMMB200_PRECISION_MIXED 1  /* FP32 arithmetic, compensated sums, FP64 geometry */
+#define FMMB200_PRECISION_MIXED 1  /* FP32 arithmetic, FP32 partials folded into FP64 sums, FP64 geometry */
 
 typedef struct fmmb200_ctx fmmb200_ctx;
 
@@ -214,7 +214,10 @@ int fmmb200_l2p(fmmb200_ctx *ctx, int32_t n, int32_t precision, int64_t npar,
 int fmmb200_direct(fmmb200_ctx *ctx, int64_t npar, const double *positions, const double *momenta,
                    double charge, double lambda, int64_t ntarget, const int64_t *targets,
                    double *efields, double *bfields);
-/* Same with device pointers (d_targets may be NULL: all particles); asynchronous. */
+/* Same with device pointers (d_targets: ntarget particle indices in [0, npar); NULL =
+ * particles 0..ntarget-1, which needs ntarget <= npar).  Returns once the kernels have
+ * finished: an index of d_targets outside [0, npar) is never read, and the call returns
+ * FMMB200_ERR_DEVICE with NaN fields for that target. */
 int fmmb200_direct_device(fmmb200_ctx *ctx, int64_t npar, const double *d_positions,
                           const double *d_momenta, double charge, double lambda, int64_t ntarget,
                           const int64_t *d_targets, double *d_efields, double *d_bfields);
@@ -225,9 +228,13 @@ int fmmb200_direct_device(fmmb200_ctx *ctx, int64_t npar, const double *d_positi
  * pool, a framework that reserved the GPU up front), where a private cudaMalloc
  * may fail or fragment that pool, and loops in which the implicit device
  * synchronisation of cudaMalloc/cudaFree is not acceptable.  The caller passes
- * device inputs and outputs (d_targets: ntarget particle indices, NULL =
- * particles 0..ntarget-1) and a cudaStream_t (NULL = default stream); the call is
- * asynchronous on it.
+ * device inputs and outputs (d_targets: ntarget particle indices in [0, npar), NULL =
+ * particles 0..ntarget-1, which needs ntarget <= npar) and a cudaStream_t (NULL =
+ * default stream); the call is asynchronous on it.  The device cannot report a bad
+ * index without a synchronisation, so an index of d_targets outside [0, npar) is not
+ * read and gives NaN fields for that target.  The call reads the CUDA error state with
+ * cudaPeekAtLastError and leaves a pending error of the caller's in place (it then
+ * returns FMMB200_ERR_CUDA without launching).
  * Scratch: a file-scope __device__ array of 6*65536 doubles (3 MiB), held by every
  * GPU that loads the library until the process exits.  ntarget > 65536 returns
  * FMMB200_ERR_CAPACITY.  The first call on a device looks up the array's device

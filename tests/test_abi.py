@@ -104,3 +104,91 @@ def test_algorithm_struct():
     assert fmmb200.FMMB200(n=4, N0=125, eta=0.5, precision="mixed").precision_code == fmmb200.PRECISION_MIXED
     with pytest.raises(ValueError):
         fmmb200.FMMB200(n=4, N0=125, eta=0.5, precision="fp16").precision_code
+
+
+JULIA = os.path.join(ROOT, "fmm4rbgpu.jl_b200", "julia", "FMMB200.jl")
+
+
+def _header_arities():
+    text = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
+    out = {}
+    for m in re.finditer(r"\b(fmmb200_[a-z0-9_]+)\s*\(([^;{]*?)\)\s*;", text):
+        params = m.group(2).strip()
+        out[m.group(1)] = 0 if params in ("", "void") else params.count(",") + 1
+    return out
+
+
+def _julia_ccalls(src):
+    """(symbol, number of argument types) of every ccall((:sym, libfmmb200), Ret, (types...), ...)."""
+    calls = []
+    for m in re.finditer(r"ccall\(\(:(fmmb200_[a-z0-9_]+),\s*libfmmb200\),\s*[A-Za-z0-9_{}]+,\s*\(", src):
+        i, depth, parts, cur = m.end(), 1, [], ""
+        while depth:
+            c = src[i]
+            if c in "({":
+                depth += 1
+            elif c in ")}":
+                depth -= 1
+            if depth == 1 and c == ",":
+                parts.append(cur)
+                cur = ""
+            elif depth:
+                cur += c
+            i += 1
+        parts.append(cur)
+        calls.append((m.group(1), len([p for p in parts if p.strip()])))
+    return calls
+
+
+def test_julia_binding_module_and_exports():
+    """The binding's module does not shadow the constructor it exports: `module FMMB200` would
+    bind FMMB200 to the module itself, so `FMMB200(0.5, 125, 4)` must come from a module of
+    another name that exports a function of that name."""
+    src = open(JULIA).read()
+    mod = re.search(r"^module\s+(\w+)", src, flags=re.M).group(1)
+    assert mod != "FMMB200"
+    assert not re.search(r"^\s*const\s+FMMB200\b", src, flags=re.M)
+    exported = set()
+    for line in re.findall(r"^export\s+(.+)$", src, flags=re.M):
+        exported |= {w.strip() for w in line.split(",")}
+    assert {"FMMB200", "FMMB200Alg", "fmm_fields"} <= exported
+    # positional (eta, N0, n) and keyword forms, both returning the struct
+    assert re.search(r"^FMMB200\(eta::Real,\s*N0::Integer,\s*n::Integer.*\)\s*=\s*\n?\s*FMMB200Alg\(", src, flags=re.M)
+    assert re.search(r"^FMMB200\(;\s*n::Integer,\s*N0::Integer,\s*eta::Real", src, flags=re.M)
+    assert re.search(r"function update_particles_field!\(p::Particles\{Float64\},\s*alg::FMMB200Alg;\s*lambda\)", src)
+
+
+def test_julia_ccalls_match_the_header():
+    src = open(JULIA).read()
+    arity = _header_arities()
+    calls = _julia_ccalls(src)
+    names = {c[0] for c in calls}
+    assert {"fmmb200_create", "fmmb200_destroy", "fmmb200_last_error", "fmmb200_update_particles_field",
+            "fmmb200_forward", "fmmb200_backward"} <= names
+    for name, nargs in calls:
+        assert name in arity, name
+        assert nargs == arity[name], (name, nargs, arity[name])
+
+
+def test_julia_rrule_reuses_pooled_contexts():
+    src = open(JULIA).read()
+    body = src[src.index("function ChainRulesCore.rrule"):]
+    body = body[: body.index("\nend\n")]
+    assert "Context(" not in body  # no new device context per differentiated call
+    assert "_acquire()" in body and "_release(ctx)" in body
+    # the error message is read before the context goes back to the pool
+    assert body.index("_error(ctx, st)") < body.index("_release(ctx)\n        err")
+
+
+def test_direct_entry_points_reject_more_targets_than_particles_without_a_list():
+    """With no target list the targets are particles 0..ntarget-1, so ntarget > npar would
+    read past the caller's buffers: both device-pointer entry points refuse it before any
+    CUDA call (the pointers are never dereferenced)."""
+    import fmmb200
+
+    lib = fmmb200.load()
+    buf = np.zeros(64)
+    p = ctypes.c_void_p(buf.ctypes.data)
+    assert lib.fmmb200_direct_noalloc(10, p, p, -1.0, 1.0, 11, None, p, p, None) == fmmb200.ERR_INVALID_ARGUMENT
+    assert lib.fmmb200_direct_noalloc(10, p, p, -1.0, 0.0, 5, None, p, p, None) == fmmb200.ERR_INVALID_ARGUMENT
+    assert lib.fmmb200_direct_device(None, 10, p, p, -1.0, 1.0, 11, None, p, p) == fmmb200.ERR_INVALID_ARGUMENT
