@@ -18,6 +18,11 @@ tree build, traversal, P2M/M2M, M2L, P2P, L2L/L2P.
   roofline the dominant kernel (M2L) against the measured CUDA-core FMA peak
   accuracy rel-L2 of mixed vs FP64 over all particles, and of both vs an FP64
            direct sum (GPU) on 4096 seeded targets
+  nsweep   the same beam at other (n, eta): mixed and FP64 ms/step and both forms'
+           rel-L2 against the FP64 direct sum, and the cheapest setting whose
+           error is <= 1e-5 (the accuracy target of the mixed form)
+  large    the N = 25,600,000 bunch of the reference's published comparison
+           (mixed, FP64, and mixed through the host-pointer call)
 
 --impl reference times the reference's algorithm on the host cores: the
 oracle's restatement of the serial FMM (parallel over targets with OpenMP,
@@ -70,7 +75,17 @@ def parse():
                          "(sigma=(0.3,0.3,0.03), u_z~N(100,0.1)); uniform: U[0,1]^3 at rest")
     ap.add_argument("--ntargets", type=int, default=4096)
     ap.add_argument("--cpu-sample", type=int, default=2**17, help="particles in the CPU-baseline sample")
-    ap.add_argument("--ref-sample", type=int, default=2**18, help="particles per reference-arm step")
+    ap.add_argument("--ref-sample", type=int, default=2**20, help="particles per reference-arm step")
+    ap.add_argument("--ref-large-sample", type=int, default=2**22,
+                    help="one more reference-arm evaluation at this size, outside the timed steps, so that "
+                         "the growth of the CPU cost per particle with N is visible (0: skip)")
+    ap.add_argument("--skip-nsweep", action="store_true")
+    ap.add_argument("--nsweep", default="2:0.5,3:0.5,4:0.5,5:0.5,6:0.5,4:0.4,4:0.3,4:0.25,4:0.2,3:0.15,4:0.15,"
+                                        "5:0.15,3:0.1,4:0.1",
+                    help="n:eta settings of the accuracy/throughput sweep (the FMM's error against the direct sum "
+                         "has a floor set by eta, from the mean momentum in its far-field kernel, so the sweep "
+                         "lowers eta rather than only raising n)")
+    ap.add_argument("--large-N", type=int, default=25_600_000, help="particles of the large line (0: skip)")
     ap.add_argument("--skip-cpu-baseline", action="store_true")
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-backward", action="store_true")
@@ -217,14 +232,25 @@ def run_reference(args, world, rank):
         times.append(time.perf_counter() - t0)
     t = sum(times) / len(times)
     v = N / t
-    sample = (f"one FMM field evaluation of a {N}-particle Gaussian bunch (same distribution, n, N0, eta) per step; "
-              f"the oracle's restatement of the reference's serial FMM (src/fmm/*.jl), OpenMP over targets")
+    # the CPU cost per particle grows with the tree depth: one evaluation at a larger size
+    by_sample = {str(N): v}
+    NL = min(args.ref_large_sample, args.N)
+    if NL > N:
+        posl, moml = generate(args, NL, args.seed)
+        t0 = time.perf_counter()
+        oracle.fmm(posl, moml, -1.0, 1.0, args.n, args.N0, args.eta, nthreads=nthreads)
+        by_sample[str(NL)] = NL / (time.perf_counter() - t0)
+        del posl, moml
+    sample = (f"one FMM field evaluation of a {N}-particle sample of the workload's distribution (same n, N0, eta) "
+              f"per step; the oracle's restatement of the reference's serial FMM (src/fmm/*.jl), OpenMP over "
+              f"targets; rate_by_sample adds one evaluation at {NL} particles")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": v, "unit": "particles/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Gaussian bunch)",
         "config": workload(args),
-        "cpu_baseline": {"value": v, "unit": "particles/s", "cores": nthreads, "kind": "port", "sample": sample},
+        "cpu_baseline": {"value": v, "unit": "particles/s", "cores": nthreads, "kind": "port", "sample": sample,
+                         "rate_by_sample": by_sample},
         "e2e": {"value": v, "unit": "particles/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
 
@@ -241,6 +267,113 @@ def cpu_baseline(args):
     return {"value": N / t, "unit": "particles/s", "cores": 1, "kind": "port",
             "sample": f"one serial FMM field evaluation (the oracle's restatement of src/fmm/*.jl, 1 thread) of a "
                       f"{N}-particle Gaussian bunch with the same distribution, n, N0 and eta; {t:.1f} s"}
+
+
+# ---------------------------------------------------------------------------- sweeps
+def _events_ms(stream, fn, steps, warmup):
+    import torch
+
+    for _ in range(warmup):
+        fn()
+    stream.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(steps):
+        fn()
+    ev1.record(stream)
+    ev1.synchronize()
+    return ev0.elapsed_time(ev1) / steps
+
+
+def run_nsweep(args, ctx, stream, N, pos, mom, tg, Ed, Bd):
+    """Both forms at each (n, eta) of --nsweep on the benchmark beam: ms/step (1 warm-up,
+    2 timed steps each) and rel-L2 of E and B on the direct sum's targets."""
+    import torch
+
+    import fmmb200
+
+    E = torch.empty_like(pos)
+    B = torch.empty_like(pos)
+
+    def rel(a, b):
+        return float(torch.linalg.norm(a - b) / torch.linalg.norm(b))
+
+    rows = []
+    for item in args.nsweep.split(","):
+        n_s, eta_s = item.split(":")
+        n, eta = int(n_s), float(eta_s)
+        row = {"n": n, "eta": eta}
+        for prec in ("mixed", "fp64"):
+            alg = fmmb200.FMMB200(n=n, N0=args.N0, eta=eta, precision=prec)
+            try:
+                ms = _events_ms(stream, lambda: ctx.forward_device(N, pos.data_ptr(), mom.data_ptr(), E.data_ptr(),
+                                                                   B.data_ptr(), alg), 2, 1)
+            except fmmb200.FMMB200Error as e:  # e.g. out of device memory at the largest n
+                row[prec] = {"error": str(e)}
+                continue
+            st = ctx.stats()
+            row[prec] = {"ms_per_step": ms, "value": N / (ms * 1e-3), "err_E": rel(E[tg], Ed), "err_B": rel(B[tg], Bd),
+                         "ms_m2l": st["ms_m2l"], "ms_p2p": st["ms_p2p"]}
+            row.update(nm2l=st["nm2l"], np2p=st["np2p"], device_bytes=st["device_bytes"])
+        if "ms_per_step" in row.get("mixed", {}) and "ms_per_step" in row.get("fp64", {}):
+            row["mixed_speedup"] = row["fp64"]["ms_per_step"] / row["mixed"]["ms_per_step"]
+        rows.append(row)
+        print(json.dumps({"nsweep_row": row}), file=sys.stderr, flush=True)
+    target = 1e-5
+    ok = [r for r in rows if "err_E" in r.get("mixed", {})
+          and max(r["mixed"]["err_E"], r["mixed"]["err_B"]) <= target]
+    best = min(ok, key=lambda r: r["mixed"]["ms_per_step"]) if ok else None
+    closest = min((r for r in rows if "err_E" in r.get("mixed", {})),
+                  key=lambda r: max(r["mixed"]["err_E"], r["mixed"]["err_B"]), default=None)
+    return {"N": N, "N0": args.N0, "targets": int(tg.numel()), "target_rel_err": target, "rows": rows,
+            "cheapest_meeting_target": None if best is None else
+            {"n": best["n"], "eta": best["eta"], "mixed_ms": best["mixed"]["ms_per_step"],
+             "mixed_value": best["mixed"]["value"], "mixed_speedup": best.get("mixed_speedup"),
+             "err_E": best["mixed"]["err_E"], "err_B": best["mixed"]["err_B"]},
+            "most_accurate": None if closest is None else {"n": closest["n"], "eta": closest["eta"],
+                                                          "err_E": closest["mixed"]["err_E"],
+                                                          "err_B": closest["mixed"]["err_B"]}}
+
+
+def run_large(args, ctx, stream, dev):
+    """The N = --large-N bunch (the reference's published comparison size) at the
+    benchmark's n, N0, eta: mixed and FP64 device-resident, mixed through the host call."""
+    import torch
+
+    import fmmb200
+
+    N = args.large_N
+    pos_h, mom_h = generate(args, N, args.seed + 11)
+    pos = torch.from_numpy(pos_h).to(dev)
+    mom = torch.from_numpy(mom_h).to(dev)
+    E = torch.empty_like(pos)
+    B = torch.empty_like(pos)
+    out = {"N": N}
+    for prec in ("mixed", "fp64"):
+        alg = fmmb200.FMMB200(n=args.n, N0=args.N0, eta=args.eta, precision=prec)
+        ms = _events_ms(stream, lambda: ctx.forward_device(N, pos.data_ptr(), mom.data_ptr(), E.data_ptr(),
+                                                           B.data_ptr(), alg), 3, 1)
+        out[prec] = {"ms_per_step": ms, "value": N / (ms * 1e-3)}
+    st = ctx.stats()
+    out.update(max_level=st["max_level"], nm2l=st["nm2l"], np2p=st["np2p"])
+    del pos, mom, E, B
+    ph = torch.from_numpy(pos_h).pin_memory()
+    mh = torch.from_numpy(mom_h).pin_memory()
+    eh = torch.empty((N, 3), dtype=torch.float64).pin_memory()
+    bh = torch.empty((N, 3), dtype=torch.float64).pin_memory()
+    dp = ctypes.POINTER(ctypes.c_double)
+    args_c = [ctypes.cast(t.data_ptr(), dp) for t in (ph, mh, eh, bh)]
+    L = ctx._lib
+
+    def host_step():
+        ctx._check(L.fmmb200_update_particles_field(ctx.handle, N, -1.0, *args_c, args.n, args.N0, args.eta, 1.0,
+                                                    fmmb200.PRECISION_MIXED))
+
+    ms = _events_ms(stream, host_step, 3, 1)
+    out["e2e_mixed"] = {"ms_per_step": ms, "value": N / (ms * 1e-3), "h2d_bytes_per_step": 48 * N,
+                        "d2h_bytes_per_step": 48 * N}
+    return out
 
 
 # ---------------------------------------------------------------------------- our arm
@@ -437,6 +570,13 @@ def run_ours(args, world, rank, local):
         e2e = {"value": replicas.aggregate_rate(world, N, ms_e2e), "unit": "particles/s", "ms_per_step": ms_e2e,
                "h2d_bytes_per_step": 2 * 24 * N, "d2h_bytes_per_step": 2 * 24 * N}
 
+    nsweep = None
+    large = None
+    if world == 1 and not args.skip_nsweep:
+        nsweep = run_nsweep(args, ctx, stream, N, pos, mom, tg, Ed, Bd)
+    if world == 1 and args.large_N > 0:
+        large = run_large(args, ctx, stream, dev)
+
     cpu = None
     if rank == 0 and world == 1 and not args.skip_cpu_baseline:
         cpu = cpu_baseline(args)
@@ -464,6 +604,8 @@ def run_ours(args, world, rank, local):
                      "torch_peak_bytes": int(torch.cuda.max_memory_allocated(dev))},
             "fwd_bwd": fwd_bwd,
             "reuse": reuse,
+            "nsweep": nsweep,
+            "large": large,
             "roofline": roof,
             "cpu_baseline": cpu,
             "e2e": e2e,

@@ -1,5 +1,7 @@
-"""The benchmark's full sizes (N = 2^24 and N = 25,600,000 Gaussian bunches), where the
-oracle cannot run: size-independent properties only.
+"""Size-independent properties at the benchmark's full sizes (N = 2^24 and N = 25,600,000
+Gaussian bunches).  The oracle comparison at these sizes (tree, lists and FP64 fields at
+N = 2^20, 2^22 and 2^24, and the direct sum) is in test_gpu_parity_fullsize.py; the checks
+here need no oracle run:
 
 * The mixed form stays within 1e-5 (relative L2 over all particles) of FP64 for n = 2..6.
 * Both forms agree with an FP64 direct sum at 4096 seeded targets to the FMM's truncation
