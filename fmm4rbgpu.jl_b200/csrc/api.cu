@@ -453,6 +453,24 @@ int download_tree(Ctx *ctx, int64_t *parindices, int64_t *levels, int64_t *parlo
 
 }  // namespace
 
+// ---- helpers of the per-rank steps of a sharded beam (shard.cu) ----------------
+namespace fmmb200 {
+
+int shard_check(Ctx *ctx, int64_t N, int n, int64_t N0, int precision) {
+  return check_common(ctx, N, n, N0, precision);
+}
+
+int shard_consts(Ctx *ctx, const double *pavg_host, double **d_consts) {
+  FMM_TRY(ctx->ensure("consts", 8, d_consts));
+  FMM_CUDA_TRY(ctx, cudaMemcpyAsync(*d_consts, pavg_host, 3 * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  stretch_kernel<<<1, 1, 0, ctx->stream>>>(*d_consts);
+  return ctx->check_launch("stretch_kernel");
+}
+
+int shard_expansions(Ctx *ctx, int n, bool mixed) { return ensure_expansions(ctx, n, mixed); }
+
+}  // namespace fmmb200
+
 // ============================================================================ exports
 extern "C" {
 

@@ -53,6 +53,9 @@ struct fmmb200_ctx {
   bool tree_reuse = false;  // forward: refit the previous tree when it is still exact
   // forward: fields of the leaves [rank nleaf / world, (rank + 1) nleaf / world) only
   int shard_rank = 0, shard_world = 1;
+  // traversal target filter of a memory-sharded rank: only the rows of the level-trav_L
+  // cluster trav_g, its descendants and its ancestors (trav_L < 0: every row)
+  int trav_L = -1, trav_g = 0;
   // the M2L target lists the M2L launchers read (a shard's compacted copy, or all)
   const char *m2l_ptr_key = "m2l_ptr";
   const char *m2l_src_key = "m2l_src";

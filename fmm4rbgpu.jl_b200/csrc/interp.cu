@@ -112,11 +112,12 @@ __global__ void __launch_bounds__(Grid<NDEG>::BT)
   }
 }
 
-// L[c][d][i][I]: weight of parent node I at coordinate d of child node i
+// L[c][d][i][I]: weight of parent node I at coordinate d of child node i, for the nch
+// children c1, c1 + 1 (nch = 1: c1 only)
 template <int M, typename T>
 __device__ __forceinline__ void transfer_weights(const double *__restrict__ nodes, int NS, int p, int c1,
-                                                 T (*L)[3][M][M]) {
-  for (int task = threadIdx.x; task < 2 * 3 * M; task += blockDim.x) {
+                                                 T (*L)[3][M][M], int nch = 2) {
+  for (int task = threadIdx.x; task < nch * 3 * M; task += blockDim.x) {
     const int ch = task / (3 * M), r = task % (3 * M), d = r / M, i = r % M;
     const int c = c1 + ch;
     const double x = nodes[(int64_t)c * NS + d * M + i];
@@ -125,9 +126,11 @@ __device__ __forceinline__ void transfer_weights(const double *__restrict__ node
 }
 
 // ---------------------------------------------------------------- M2M
+// The tree is a heap stored from cluster `off` on (off = 0: the whole tree; a sharded
+// rank keeps the top levels of the beam's tree at an offset).
 template <int NDEG, bool MIXED>
 __global__ void __launch_bounds__(Grid<NDEG>::BT)
-    m2m_kernel(int plevel, const double *__restrict__ nodes, void *__restrict__ mom_v, int accumulate) {
+    m2m_kernel(int plevel, int off, const double *__restrict__ nodes, void *__restrict__ mom_v, int accumulate) {
   using Gd = Grid<NDEG>;
   constexpr int M = Gd::M, NN = Gd::NN, NS = Gd::NS, BT = Gd::BT, NPT = Gd::NPT;
   using T = typename std::conditional<MIXED, float, double>::type;
@@ -138,8 +141,8 @@ __global__ void __launch_bounds__(Grid<NDEG>::BT)
   T *s_t2 = s_t1 + 4 * NN;  // 4*NN
   T *mom = (T *)mom_v;
   const int tid = threadIdx.x;
-  const int p = (1 << plevel) - 1 + blockIdx.x;
-  const int c1 = 2 * p + 1;
+  const int p = off + (1 << plevel) - 1 + blockIdx.x;
+  const int c1 = off + 2 * (p - off) + 1;
   transfer_weights<M, T>(nodes, NS, p, c1, L);
   T acc[NPT][4];
 #pragma unroll
@@ -202,11 +205,14 @@ __global__ void __launch_bounds__(Grid<NDEG>::BT)
 }
 
 // ---------------------------------------------------------------- L2L
-// One CTA per parent at level clevel-1; both children receive
+// One CTA per parent at level clevel-1 of the heap stored from cluster `off`; both
+// children receive
 // child[q][i + M(j + Mk)] += sum_{IJK} parent[q][I + M(J + MK)] Lx[i][I] Ly[j][J] Lz[k][K].
+// With pc given, CTA b instead transfers parent pc[b].x into the one child pc[b].y.
 template <int NDEG, bool MIXED>
 __global__ void __launch_bounds__(Grid<NDEG>::BT)
-    l2l_kernel(int clevel, const double *__restrict__ nodes, void *__restrict__ loc_v) {
+    l2l_kernel(int clevel, int off, const int2 *__restrict__ pc, const double *__restrict__ nodes,
+               void *__restrict__ loc_v) {
   using Gd = Grid<NDEG>;
   constexpr int M = Gd::M, NN = Gd::NN, NS = Gd::NS, BT = Gd::BT;
   using T = typename std::conditional<MIXED, float, double>::type;
@@ -217,15 +223,16 @@ __global__ void __launch_bounds__(Grid<NDEG>::BT)
   T *s_t2 = s_t1 + 6 * NN;    // 6*NN
   T *loc = (T *)loc_v;
   const int tid = threadIdx.x;
-  const int p = (1 << (clevel - 1)) - 1 + blockIdx.x;
-  const int c1 = 2 * p + 1;
-  transfer_weights<M, T>(nodes, NS, p, c1, L);
+  const int p = pc ? pc[blockIdx.x].x : off + (1 << (clevel - 1)) - 1 + blockIdx.x;
+  const int c1 = pc ? pc[blockIdx.x].y : off + 2 * (p - off) + 1;
+  const int nch = pc ? 1 : 2;
+  transfer_weights<M, T>(nodes, NS, p, c1, L, nch);
   const T *pl = loc + (int64_t)p * 6 * NN;
   for (int e = tid; e < 6 * NN; e += BT) s_par[e] = pl[e];
   __syncthreads();
   // all six quantities per stage; the z stage of one child reads only t2, which the
   // next child's y stage rewrites after the barrier that follows its x stage
-  for (int ch = 0; ch < 2; ++ch) {
+  for (int ch = 0; ch < nch; ++ch) {
     T *cl = loc + (int64_t)(c1 + ch) * 6 * NN;
     // x: t1[q][i + M(J + MK)] = sum_I Lx[i][I] par[q][I + M(J + MK)]
     for (int e = tid; e < 6 * NN; e += BT) {
@@ -389,21 +396,24 @@ struct Launch {
         MIXED ? (void *)ctx->get<float>("mom32") : (void *)ctx->get<double>("mom64"), accumulate ? 1 : 0);
     return ctx->check_launch("p2m_kernel");
   }
-  static int m2m(Ctx *ctx, int plevel, bool accumulate) {
+  static int m2m(Ctx *ctx, int plevel, bool accumulate, int off = 0) {
     const int smem = 3 * 4 * Gd::NN * (int)sizeof(T);
     auto k = m2m_kernel<NDEG, MIXED>;
     FMM_TRY(opt_in_smem(ctx, k, smem));
     k<<<1u << plevel, Gd::BT, smem, ctx->stream>>>(
-        plevel, ctx->get<double>("nodes"),
+        plevel, off, ctx->get<double>("nodes"),
         MIXED ? (void *)ctx->get<float>("mom32") : (void *)ctx->get<double>("mom64"), accumulate ? 1 : 0);
     return ctx->check_launch("m2m_kernel");
   }
-  static int l2l(Ctx *ctx, int clevel) {
+  static int l2l(Ctx *ctx, int clevel, int off = 0, const int2 *pc = nullptr, int npc = 0) {
     const int smem = 18 * Gd::NN * (int)sizeof(T);
     auto k = l2l_kernel<NDEG, MIXED>;
     FMM_TRY(opt_in_smem(ctx, k, smem));
-    k<<<1u << (clevel - 1), Gd::BT, smem, ctx->stream>>>(
-        clevel, ctx->get<double>("nodes"), MIXED ? (void *)ctx->get<float>("loc32") : (void *)ctx->get<double>("loc64"));
+    const unsigned grid = pc ? (unsigned)npc : 1u << (clevel - 1);
+    if (grid == 0) return FMMB200_OK;
+    k<<<grid, Gd::BT, smem, ctx->stream>>>(
+        clevel, off, pc, ctx->get<double>("nodes"),
+        MIXED ? (void *)ctx->get<float>("loc32") : (void *)ctx->get<double>("loc64"));
     return ctx->check_launch("l2l_kernel");
   }
   static int l2p(Ctx *ctx, const int *ids, int64_t nleaf, int mode, double amp, double *oe, double *ob) {
@@ -444,6 +454,15 @@ int launch_m2m(Ctx *ctx, int n, bool mixed, int plevel, bool accumulate) {
   FMM_DISPATCH(n, mixed, m2m(ctx, plevel, accumulate))
 }
 int launch_l2l(Ctx *ctx, int n, bool mixed, int clevel) { FMM_DISPATCH(n, mixed, l2l(ctx, clevel)) }
+int launch_m2m_heap(Ctx *ctx, int n, bool mixed, int plevel, int off) {
+  FMM_DISPATCH(n, mixed, m2m(ctx, plevel, false, off))
+}
+int launch_l2l_heap(Ctx *ctx, int n, bool mixed, int clevel, int off) {
+  FMM_DISPATCH(n, mixed, l2l(ctx, clevel, off))
+}
+int launch_l2l_pairs(Ctx *ctx, int n, bool mixed, const int2 *d_pc, int npc) {
+  FMM_DISPATCH(n, mixed, l2l(ctx, 1, 0, d_pc, npc))
+}
 int launch_l2p(Ctx *ctx, int n, bool mixed, const int *ids, int64_t nleaf, int mode, double amp, double *oe,
                double *ob) {
   FMM_DISPATCH(n, mixed, l2p(ctx, ids, nleaf, mode, amp, oe, ob))

@@ -33,9 +33,10 @@ int compute_pavg_stretch(Ctx *ctx, const double *d_mom_aos, int64_t N, double *d
 // Build the cluster tree of N particles (AoS positions on device) with the
 // stretch in d_consts[3..5]; fills ctx tree buffers and ctx->{N,N0,ml,nc,...}.
 // after_sorts, if given, is called once the three coordinate orders are sorted and
-// before anything reads d_consts (the radix sorts need the positions only).
+// before anything reads d_consts (the radix sorts need the positions only).  depth >= 0
+// replaces the maximum level computed from N and N0 (the shape rules still apply).
 int build_tree(Ctx *ctx, const double *d_pos_aos, int64_t N, int64_t N0, const double *d_consts,
-               const std::function<int()> &after_sorts = {});
+               const std::function<int()> &after_sorts = {}, int depth = -1);
 // Refit the existing tree (same N, N0) to new positions: boxes and extremal
 // particles bottom-up, and *same = true when every node would split as before, in
 // which case the tree equals what build_tree would give.  Otherwise the refitted
@@ -55,6 +56,9 @@ int compute_nodes(Ctx *ctx, int n);
 int node_stride(int n);
 
 // ---------------------------------------------------------------- traverse.cu
+// Device buffer `name` of at least `need` bytes whose first `used` bytes survive a
+// reallocation (which leaves headroom, so that similar later needs grow nothing).
+int grow_keep(Ctx *ctx, const char *name, size_t used, size_t need, void **out);
 int build_lists(Ctx *ctx, double eta, const double *d_consts);
 // m2lu_* / p2pu_*: union of each list and its transpose with role flags
 // (bit 0: (t,s) in the list, bit 1: (s,t) in the list), grouped by target.
@@ -72,6 +76,11 @@ int launch_p2m(Ctx *ctx, int n, bool mixed, const int *d_leaf_ids, int64_t nleaf
 int launch_m2m(Ctx *ctx, int n, bool mixed, int plevel, bool accumulate);
 // L2L for all children at child level `clevel` (>= 1).
 int launch_l2l(Ctx *ctx, int n, bool mixed, int clevel);
+// The same two passes on a heap of clusters stored from cluster `off` on.
+int launch_m2m_heap(Ctx *ctx, int n, bool mixed, int plevel, int off);
+int launch_l2l_heap(Ctx *ctx, int n, bool mixed, int clevel, int off);
+// L2L from parent d_pc[b].x into the single child d_pc[b].y, b < npc.
+int launch_l2l_pairs(Ctx *ctx, int n, bool mixed, const int2 *d_pc, int npc);
 // L2P of leaves.  mode 0: explicit (near += far at tree-order particles);
 // mode 1: pipeline (out_aos[perm] = amp * (near + far)).
 int launch_l2p(Ctx *ctx, int n, bool mixed, const int *d_leaf_ids, int64_t nleaf, int mode,
@@ -80,5 +89,12 @@ int launch_l2p(Ctx *ctx, int n, bool mixed, const int *d_leaf_ids, int64_t nleaf
 // ---------------------------------------------------------------- m2l.cu / p2p.cu
 int launch_m2l(Ctx *ctx, int n, bool mixed, bool accumulate);
 int launch_p2p(Ctx *ctx, bool mixed, const int *d_leaf_ids, int64_t nleaf, bool accumulate);
+
+// ---------------------------------------------------------------- api.cu, for shard.cu
+// Argument checks of a forward; consts[0..5] = (p_avg, stretch) from a host p_avg; the
+// moment / local / near-field buffers of the context's tree.
+int shard_check(Ctx *ctx, int64_t N, int n, int64_t N0, int precision);
+int shard_consts(Ctx *ctx, const double *pavg_host, double **d_consts);
+int shard_expansions(Ctx *ctx, int n, bool mixed);
 
 }  // namespace fmmb200

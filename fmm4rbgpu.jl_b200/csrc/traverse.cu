@@ -24,6 +24,21 @@ constexpr int kTvTile = kTvThreads * kTvItems;
 
 enum : int { kCatP2P = 0, kCatM2L = 1, kCatSplit = 2 };
 
+// Target filter of a sharded traversal (TravFilter::L < 0: every target).  A rank that
+// owns the level-L cluster g (heap id) needs the rows of g's descendants and of g's
+// ancestors only; a split whose target child is neither drops that child pair.
+struct TravFilter {
+  int L;
+  int g;
+};
+
+__device__ __forceinline__ bool trav_relevant(int t, TravFilter f) {
+  if (f.L < 0) return true;
+  const int lt = 31 - __clz(t + 1);
+  if (lt <= f.L) return ((f.g + 1) >> (f.L - lt)) == t + 1;  // t is g or an ancestor of g
+  return ((t + 1) >> (lt - f.L)) == f.g + 1;                  // t is below g
+}
+
 // Returns the category; for a split, (*ct1,*cs1),(*ct2,*cs2) are the child pairs.
 __device__ __forceinline__ int classify(const ClusterGeom *__restrict__ geom, int t, int s, double s0, double s1,
                                         double s2, double eta, int *ct1, int *cs1, int *ct2, int *cs2) {
@@ -55,8 +70,10 @@ __device__ __forceinline__ int classify(const ClusterGeom *__restrict__ geom, in
   return kCatSplit;
 }
 
+// Counts per block: P2P pairs, M2L pairs and the child pairs of the splits (two per
+// split, fewer when the target filter drops one).
 __global__ void trav_count_kernel(const int2 *__restrict__ front, int nf, const ClusterGeom *__restrict__ geom,
-                                  const double *__restrict__ consts, double eta, int nblk,
+                                  const double *__restrict__ consts, double eta, int nblk, TravFilter flt,
                                   int *__restrict__ bcount, int *__restrict__ totals) {
   __shared__ int s_warp[33];
   const double s0 = consts[3], s1 = consts[4], s2 = consts[5];
@@ -67,7 +84,11 @@ __global__ void trav_count_kernel(const int2 *__restrict__ front, int nf, const 
     if (q < nf) {
       int2 p = front[q];
       int a, b, cc, d;
-      c[classify(geom, p.x, p.y, s0, s1, s2, eta, &a, &b, &cc, &d)]++;
+      const int cat = classify(geom, p.x, p.y, s0, s1, s2, eta, &a, &b, &cc, &d);
+      if (cat == kCatSplit)
+        c[2] += (int)trav_relevant(a, flt) + (int)trav_relevant(cc, flt);
+      else
+        c[cat]++;
     }
   }
   for (int k = 0; k < 3; ++k) {
@@ -81,7 +102,7 @@ __global__ void trav_count_kernel(const int2 *__restrict__ front, int nf, const 
 }
 
 __global__ void trav_write_kernel(const int2 *__restrict__ front, int nf, const ClusterGeom *__restrict__ geom,
-                                  const double *__restrict__ consts, double eta, int nblk,
+                                  const double *__restrict__ consts, double eta, int nblk, TravFilter flt,
                                   const int *__restrict__ boff, int bits, uint64_t *__restrict__ p2p,
                                   uint64_t *__restrict__ m2l, int2 *__restrict__ next) {
   __shared__ int s_warp[33];
@@ -96,7 +117,10 @@ __global__ void trav_write_kernel(const int2 *__restrict__ front, int nf, const 
     if (q < nf) {
       pr[i] = front[q];
       cat[i] = classify(geom, pr[i].x, pr[i].y, s0, s1, s2, eta, &ch1[i].x, &ch1[i].y, &ch2[i].x, &ch2[i].y);
-      c[cat[i]]++;
+      if (cat[i] == kCatSplit)
+        c[2] += (int)trav_relevant(ch1[i].x, flt) + (int)trav_relevant(ch2[i].x, flt);
+      else
+        c[cat[i]]++;
     }
   }
   int pos[3];
@@ -110,9 +134,8 @@ __global__ void trav_write_kernel(const int2 *__restrict__ front, int nf, const 
     } else if (cat[i] == kCatM2L) {
       m2l[pos[1]++] = key;
     } else {
-      int o = pos[2]++;
-      next[2 * o] = ch1[i];
-      next[2 * o + 1] = ch2[i];
+      if (trav_relevant(ch1[i].x, flt)) next[pos[2]++] = ch1[i];
+      if (trav_relevant(ch2[i].x, flt)) next[pos[2]++] = ch2[i];
     }
   }
 }
@@ -184,37 +207,6 @@ __global__ void union_compact_kernel(const uint64_t *__restrict__ u, int64_t n, 
   uflag[pos[i]] = (uint8_t)f;
 }
 
-// Grow a device buffer keeping its first `used` bytes.
-int grow_keep(Ctx *ctx, const char *name, size_t used, size_t need, void **out) {
-  auto it = ctx->bufs.find(name);
-  if (it != ctx->bufs.end() && it->second.cap >= need) {
-    *out = it->second.p;
-    return FMMB200_OK;
-  }
-  void *fresh = nullptr;
-  size_t want = need + need / 2;
-  want = (want + 255) & ~(size_t)255;
-  if (ctx->fail_alloc_countdown > 0 && --ctx->fail_alloc_countdown == 0)
-    return ctx->fail(FMMB200_ERR_OUT_OF_MEMORY, std::string("injected allocation failure for buffer '") + name + "'");
-  cudaError_t e = cudaMalloc(&fresh, want);
-  if (e != cudaSuccess) {
-    cudaGetLastError();
-    return ctx->fail(FMMB200_ERR_OUT_OF_MEMORY, std::string("cudaMalloc for '") + name + "': " + cudaGetErrorString(e));
-  }
-  if (it != ctx->bufs.end() && it->second.p) {
-    if (used) FMM_CUDA_TRY(ctx, cudaMemcpyAsync(fresh, it->second.p, used, cudaMemcpyDeviceToDevice, ctx->stream));
-    FMM_TRY(ctx->sync());
-    cudaFree(it->second.p);
-    ctx->device_bytes -= it->second.cap;
-  }
-  auto &b = ctx->bufs[name];
-  b.p = fresh;
-  b.cap = want;
-  ctx->device_bytes += want;
-  *out = fresh;
-  return FMMB200_OK;
-}
-
 int sort_and_group(Ctx *ctx, const char *keys_name, const char *alt_name, const char *ptr_name,
                    const char *src_name, int64_t n, int bits) {
   uint64_t *keys = ctx->get<uint64_t>(keys_name), *alt = nullptr;
@@ -275,6 +267,37 @@ int build_union(Ctx *ctx, const char *keys_name, int64_t n, const char *prefix) 
 
 }  // namespace
 
+// Grow a device buffer keeping its first `used` bytes.
+int grow_keep(Ctx *ctx, const char *name, size_t used, size_t need, void **out) {
+  auto it = ctx->bufs.find(name);
+  if (it != ctx->bufs.end() && it->second.cap >= need) {
+    *out = it->second.p;
+    return FMMB200_OK;
+  }
+  void *fresh = nullptr;
+  size_t want = need + need / 2;
+  want = (want + 255) & ~(size_t)255;
+  if (ctx->fail_alloc_countdown > 0 && --ctx->fail_alloc_countdown == 0)
+    return ctx->fail(FMMB200_ERR_OUT_OF_MEMORY, std::string("injected allocation failure for buffer '") + name + "'");
+  cudaError_t e = cudaMalloc(&fresh, want);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return ctx->fail(FMMB200_ERR_OUT_OF_MEMORY, std::string("cudaMalloc for '") + name + "': " + cudaGetErrorString(e));
+  }
+  if (it != ctx->bufs.end() && it->second.p) {
+    if (used) FMM_CUDA_TRY(ctx, cudaMemcpyAsync(fresh, it->second.p, used, cudaMemcpyDeviceToDevice, ctx->stream));
+    FMM_TRY(ctx->sync());
+    cudaFree(it->second.p);
+    ctx->device_bytes -= it->second.cap;
+  }
+  auto &b = ctx->bufs[name];
+  b.p = fresh;
+  b.cap = want;
+  ctx->device_bytes += want;
+  *out = fresh;
+  return FMMB200_OK;
+}
+
 int build_union_lists(Ctx *ctx) {
   FMM_TRY(build_union(ctx, "m2l_keys", ctx->nm2l, "m2lu"));
   FMM_TRY(build_union(ctx, "p2p_keys", ctx->np2p, "p2pu"));
@@ -303,30 +326,32 @@ int build_lists(Ctx *ctx, double eta, const double *d_consts) {
   int64_t nf = 1, np2p = 0, nm2l = 0;
   int steps = 0;
   const ClusterGeom *geom = ctx->get<ClusterGeom>("geom");
+  const TravFilter flt{ctx->trav_L, ctx->trav_g};
   while (nf > 0) {
     const int nblk = ceil_div(nf, kTvTile);
     FMM_TRY(ctx->ensure("trav_bcount", 3 * (int64_t)nblk, &bcount));
     FMM_TRY(ctx->ensure("trav_boff", 3 * (int64_t)nblk, &boff));
     FMM_CUDA_TRY(ctx, cudaMemsetAsync(totals, 0, sizeof(int) * 4, ctx->stream));
-    trav_count_kernel<<<nblk, kTvThreads, 0, ctx->stream>>>(fa, (int)nf, geom, d_consts, eta, nblk, bcount, totals);
+    trav_count_kernel<<<nblk, kTvThreads, 0, ctx->stream>>>(fa, (int)nf, geom, d_consts, eta, nblk, flt, bcount,
+                                                             totals);
     FMM_TRY(ctx->check_launch("trav_count_kernel"));
     FMM_TRY(exclusive_scan_i32(ctx, bcount, boff, 3 * (int64_t)nblk, nullptr));
     FMM_TRY(ctx->pinned(sizeof(int) * 4, (void **)&h));
     FMM_CUDA_TRY(ctx, cudaMemcpyAsync(h, totals, sizeof(int) * 3, cudaMemcpyDeviceToHost, ctx->stream));
     FMM_TRY(ctx->sync());
-    const int64_t tp = h[0], tm = h[1], ts = h[2];
+    const int64_t tp = h[0], tm = h[1], tc = h[2];  // tc: child pairs of the next frontier
     FMM_TRY(grow_keep(ctx, "p2p_keys", sizeof(uint64_t) * np2p, sizeof(uint64_t) * (np2p + tp), &vp));
     p2p = (uint64_t *)vp;
     FMM_TRY(grow_keep(ctx, "m2l_keys", sizeof(uint64_t) * nm2l, sizeof(uint64_t) * (nm2l + tm), &vp));
     m2l = (uint64_t *)vp;
-    FMM_TRY(ctx->ensure("front_b", 2 * ts + 1, &fb));  // destination: contents not needed
-    if (2 * ts + 1 > front_need) front_need = 2 * ts + 1;
-    trav_write_kernel<<<nblk, kTvThreads, 0, ctx->stream>>>(fa, (int)nf, geom, d_consts, eta, nblk, boff, bits,
-                                                             p2p + np2p, m2l + nm2l, fb);
+    FMM_TRY(ctx->ensure("front_b", tc + 1, &fb));  // destination: contents not needed
+    if (tc + 1 > front_need) front_need = tc + 1;
+    trav_write_kernel<<<nblk, kTvThreads, 0, ctx->stream>>>(fa, (int)nf, geom, d_consts, eta, nblk, flt, boff,
+                                                             bits, p2p + np2p, m2l + nm2l, fb);
     FMM_TRY(ctx->check_launch("trav_write_kernel"));
     np2p += tp;
     nm2l += tm;
-    nf = 2 * ts;
+    nf = tc;
     std::swap(ctx->bufs["front_a"], ctx->bufs["front_b"]);
     fa = ctx->get<int2>("front_a");
     fb = ctx->get<int2>("front_b");

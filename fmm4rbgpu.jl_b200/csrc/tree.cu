@@ -710,11 +710,13 @@ int compute_pavg_stretch(Ctx *ctx, const double *d_mom, int64_t N, double *d_con
 }
 
 int build_tree(Ctx *ctx, const double *d_pos, int64_t N64, int64_t N0, const double *d_consts,
-               const std::function<int()> &after_sorts) {
+               const std::function<int()> &after_sorts, int depth) {
   if (N64 > 0x7FFFFFFF) return ctx->fail(FMMB200_ERR_INVALID_ARGUMENT, "npar must be < 2^31");
   const int N = (int)N64;
-  // tree shape (treeinfo.jl:6-26) with the reference's floating-point formula
+  // tree shape (treeinfo.jl:6-26) with the reference's floating-point formula, unless the
+  // depth is given (the subtree of a sharded beam has the whole tree's remaining depth)
   int ml = N > N0 ? (int)std::ceil(std::log((double)N / (double)N0) / std::log(2.0)) : 0;
+  if (depth >= 0) ml = depth;
   if (ml > 29) return ctx->fail(FMMB200_ERR_INVALID_ARGUMENT, "tree depth > 29 (N0 too small for npar)");
   // every level-ml node must be a leaf and every node above must split
   int64_t maxc_ml = (N64 + ((int64_t)1 << ml) - 1) >> ml;

@@ -19,7 +19,8 @@ LIB_DIR = os.path.join(PKG_ROOT, "lib")
 LIB_PATH = os.path.join(LIB_DIR, "libfmmb200.so")
 INCLUDE = os.path.join(os.path.dirname(PKG_ROOT), "include")
 
-SOURCES = ["sort.cu", "tree.cu", "traverse.cu", "interp.cu", "m2l.cu", "p2p.cu", "backward.cu", "direct.cu", "api.cu"]
+SOURCES = ["sort.cu", "tree.cu", "traverse.cu", "interp.cu", "m2l.cu", "p2p.cu", "backward.cu", "direct.cu", "api.cu",
+           "shard.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2", "-diag-suppress", "177"]
 

@@ -109,6 +109,15 @@ SIGNATURES = {
     "fmmb200_set_tree_reuse": (ctypes.c_int, [c_vp, ctypes.c_int]),
     "fmmb200_set_shard": (ctypes.c_int, [c_vp, ctypes.c_int, ctypes.c_int]),
     "fmmb200_direct_noalloc": (ctypes.c_int, [c_i64, c_vp, c_vp, c_f64, c_f64, c_i64, c_vp, c_vp, c_vp, c_vp]),
+    "fmmb200_shard_record_bytes": (ctypes.c_int, [c_i32, c_i32, p_i64, p_i64]),
+    "fmmb200_shard_subtree": (ctypes.c_int, [c_vp, c_i64, c_vp, c_vp, c_i64, c_i32, p_f64, c_i32, c_i32]),
+    "fmmb200_shard_boxes": (ctypes.c_int, [c_vp, c_vp]),
+    "fmmb200_shard_pack": (ctypes.c_int, [c_vp, c_i64, c_vp, c_vp, c_i64, c_vp, c_vp, c_vp]),
+    "fmmb200_shard_lists": (ctypes.c_int, [c_vp, c_i64, c_i32, c_vp, p_f64, c_f64, c_i32, c_i32, p_i64]),
+    "fmmb200_shard_get_lists": (ctypes.c_int, [c_vp, c_vp, c_vp, c_vp, c_vp]),
+    "fmmb200_shard_evaluate": (ctypes.c_int, [c_vp, c_i32, c_i32, c_i64, c_f64, c_i64, c_vp, c_vp, c_vp, c_i64,
+                                              c_vp, c_vp, c_vp, c_i64, c_vp, c_vp, c_i64, c_f64, c_f64, c_vp,
+                                              c_vp]),
 }
 
 

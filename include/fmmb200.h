@@ -245,6 +245,60 @@ int fmmb200_direct_device(fmmb200_ctx *ctx, int64_t npar, const double *d_positi
 int fmmb200_direct_noalloc(int64_t npar, const double *d_positions, const double *d_momenta,
                            double charge, double lambda, int64_t ntarget, const int64_t *d_targets,
                            double *d_efields, double *d_bfields, void *stream);
+/* ---- one beam over several GPUs, each holding part of the tree ------------------
+ * No counterpart in the reference, whose FMMGPU evaluates the whole beam on one device
+ * (src/update_particles_field.jl:66-148; its tree is built by ClusterTree,
+ * src/cluster_tree/cluster_tree.jl:12-18, and traversed by dualtraversefill!,
+ * src/fmm/interaction_lists.jl:23-49).  With 2^L ranks the tree is split at level L:
+ * the caller partitions the first L levels across the ranks exactly as ClusterTree
+ * would (the left child takes the first ceil(cnt/2) particles in (coordinate, index)
+ * order along argmax(stretch .* extent)), so rank r holds the particles of the level-L
+ * cluster g = 2^L - 1 + r, in ascending global index order.  Then, per rank (device
+ * pointers, on the context stream, returning after the work is done):
+ *   shard_subtree   builds g's subtree with `depth` = the whole tree's max level - L
+ *                   levels and the given p_avg (HOST double[3], the whole beam's), and
+ *                   computes its moments (P2M, M2M);
+ *   shard_boxes     its nc_sub = 2^(depth+1) - 1 boxes (double[6 nc_sub], subtree heap
+ *                   order), for the caller to all-gather into the whole tree's boxes;
+ *   shard_lists     the dual traversal of the whole tree (nc = 2^(max_level+1) - 1 boxes in
+ *                   heap order) keeping the rows of g's subtree and g's ancestors only
+ *                   (counts = {nm2l, np2p}); shard_get_lists copies them out as CSR over
+ *                   the nc targets (whole-tree cluster ids, sources ascending per row);
+ *   shard_pack      moment records of the listed subtree clusters and particle records of
+ *                   the listed subtree leaves (leaf k's records from record
+ *                   d_leaf_offsets[k] on), which other ranks need;
+ *   shard_evaluate  the fields of its own particles.  Local cluster numbers are: the
+ *                   subtree (0 .. nc_sub-1), then `next` appended clusters: first the
+ *                   whole tree's top 2^(L+1) - 1 clusters in heap order (level L: every
+ *                   rank's subtree root, with its moments; above: computed here), then
+ *                   remote clusters.  d_lohi_ext gives each appended cluster's range in
+ *                   the nhalo appended particle records (hi < lo: none).  The lists are
+ *                   CSR over the nc_sub + next local clusters, rows in the whole tree's
+ *                   order.  max_leaf is the whole tree's largest leaf.  Fields go to the
+ *                   own particles in the order shard_subtree received them.
+ * Record sizes: shard_record_bytes (moments: 4 (n+1)^3 values of the precision's type;
+ * particles: 64 bytes FP64, 80 bytes mixed).  The fields equal the single-GPU forward's
+ * with the same p_avg bit for bit.  No adjoint is kept. */
+int fmmb200_shard_record_bytes(int32_t n, int32_t precision, int64_t *moment_record,
+                               int64_t *particle_record);
+int fmmb200_shard_subtree(fmmb200_ctx *ctx, int64_t npar, const double *d_positions,
+                          const double *d_momenta, int64_t N0, int32_t depth, const double *pavg,
+                          int32_t n, int32_t precision);
+int fmmb200_shard_boxes(fmmb200_ctx *ctx, double *d_bboxes);
+int fmmb200_shard_pack(fmmb200_ctx *ctx, int64_t nclusters, const int32_t *d_cluster_ids,
+                       void *d_moments, int64_t nleaves, const int32_t *d_leaf_ids,
+                       const int64_t *d_leaf_offsets, void *d_records);
+int fmmb200_shard_lists(fmmb200_ctx *ctx, int64_t nc, int32_t max_level, const double *d_bboxes,
+                        const double *pavg, double eta, int32_t L, int32_t rank, int64_t *counts);
+int fmmb200_shard_get_lists(fmmb200_ctx *ctx, int32_t *d_m2l_ptr, int32_t *d_m2l_src,
+                            int32_t *d_p2p_ptr, int32_t *d_p2p_src);
+int fmmb200_shard_evaluate(fmmb200_ctx *ctx, int32_t L, int32_t rank, int64_t max_leaf, double eta,
+                           int64_t next, const double *d_bboxes_ext, const void *d_moments_ext,
+                           const int32_t *d_lohi_ext, int64_t nhalo, const void *d_halo_records,
+                           const int32_t *d_m2l_ptr, const int32_t *d_m2l_src, int64_t nm2l,
+                           const int32_t *d_p2p_ptr, const int32_t *d_p2p_src, int64_t np2p,
+                           double charge, double lambda, double *d_efields, double *d_bfields);
+
 /* Measured CUDA-core FMA throughput (TFLOP/s, 2 flops per FMA) of the device with
  * scalar FP64, scalar FP32 and packed FP32x2 (FFMA2) chains: the roofline
  * denominators of the M2L / P2P kernels. */

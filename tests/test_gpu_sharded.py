@@ -1,11 +1,17 @@
-"""The sharded forward (fmmb200_set_shard) on the GPU.
+"""One beam over several GPUs on the GPU.
 
-* One process: the shards' fields add up to the unsharded forward bit for bit, every
-  particle's field comes from exactly one shard, for FP64 and the mixed form, for shard
-  counts that do and do not divide the number of leaves, and with more shards than
-  leaves.
+* The leaf-range shards of fmmb200_set_shard (every rank holds the whole tree): in one
+  process they add up to the unsharded forward bit for bit, every particle's field coming
+  from exactly one shard, for FP64 and the mixed form, for shard counts that do and do not
+  divide the number of leaves, and with more shards than leaves.
+* The memory-sharded forward (fmmb200.sharded: the tree split at level log2(ranks), each
+  rank holding its subtree, the whole tree's boxes and the halo it receives): 2, 4 and 8
+  ranks in one process (LoopbackComm, the ranks evaluated in turn) give the single-GPU
+  forward's fields with the same p_avg bit for bit, FP64 and mixed, Gaussian bunch and
+  beamlets, eta below and above 1/2, ranks with different numbers of particles (none, for
+  one); each rank holds far less device memory than the single-GPU forward.
 * Two processes on the one GPU joined by gloo (fmmb200.sharded.sharded_fields): each gets
-  the unsharded fields of its own particles bit for bit.  Their kernels never wait on each
+  the single-GPU fields of its own particles bit for bit.  Their kernels never wait on each
   other; the exchange runs on host copies.
 """
 import os
@@ -80,6 +86,91 @@ def test_shard_arguments_and_adjoint_are_checked(gpu_ctx):
         gpu_ctx.set_shard(0, 1)
 
 
+def _slots(pos, mom, counts):
+    import torch
+
+    import fmmb200
+
+    out, lo = [], 0
+    for c in counts:
+        out.append(dict(pos=torch.tensor(pos[lo:lo + c], device="cuda"), mom=torch.tensor(mom[lo:lo + c], device="cuda"),
+                        ctx=fmmb200.Context(0), ctx_lists=fmmb200.Context(0)))
+        lo += c
+    return out
+
+
+@pytest.mark.parametrize("world,counts,kind,n,N0,eta,precision", [
+    (2, [40000, 20000], "gauss", 4, 64, 0.5, "fp64"),
+    (2, [40000, 20000], "gauss", 4, 64, 0.5, "mixed"),
+    (4, [0, 30000, 17000, 13000], "gauss", 3, 50, 0.5, "mixed"),
+    (8, [7500] * 8, "beamlets", 5, 64, 0.5, "mixed"),
+    (8, [9000, 0, 11000, 7000, 8000, 5000, 9000, 11000], "gauss", 4, 40, 0.6, "fp64"),
+    (4, [20000, 20000, 10000, 10000], "uniform", 4, 64, 0.5, "mixed"),
+])
+def test_memory_sharded_forward_equals_the_single_gpu_forward(gpu_ctx, world, counts, kind, n, N0, eta, precision):
+    import fmmb200
+    from fmmb200 import beams, sharded
+
+    pos, mom = {"gauss": beams.gaussian_bunch, "beamlets": beams.beamlets, "uniform": beams.uniform}[kind](
+        sum(counts), seed=9)
+    alg = fmmb200.FMMB200(n=n, N0=N0, eta=eta, precision=precision)
+    slots = _slots(pos, mom, counts)
+    try:
+        out = sharded.forward_slots(sharded.LoopbackComm(world), slots, alg, charge=-1.0, lambda_=2.0)
+        pavg = slots[0]["info"]["pavg"]
+        assert all(s["info"]["pavg"] == pavg for s in slots)
+        with fmmb200.Context(0) as one:
+            E, B = one.forward(pos, mom, alg, charge=-1.0, lambda_=2.0, p_avg=pavg)
+            single_bytes = one.stats()["device_bytes"]
+        Es = np.concatenate([e.cpu().numpy() for e, _ in out])
+        Bs = np.concatenate([b.cpu().numpy() for _, b in out])
+        assert np.array_equal(Es, E) and np.array_equal(Bs, B)
+        for s in slots:
+            assert s["info"]["device_bytes"] + s["info"]["list_device_bytes"] < single_bytes
+    finally:
+        for s in slots:
+            s["ctx"].close()
+            s["ctx_lists"].close()
+
+
+def test_memory_sharded_lists_are_checked(gpu_ctx):
+    """shard_evaluate refuses lists that point outside the local clusters or records."""
+    import ctypes
+
+    import torch
+
+    import fmmb200
+    from fmmb200 import beams
+
+    pos, mom = beams.gaussian_bunch(5000, seed=3)
+    with fmmb200.Context(0) as ctx:
+        L = ctx._lib
+        dp = torch.tensor(pos, device="cuda")
+        dm = torch.tensor(mom, device="cuda")
+        pa = np.array([0.0, 0.0, 200.0])
+        ctx._check(L.fmmb200_shard_subtree(ctx.handle, 5000, ctypes.c_void_p(dp.data_ptr()),
+                                           ctypes.c_void_p(dm.data_ptr()), 50, 7, pa.ctypes.data_as(fmmb200._lib.p_f64),
+                                           3, fmmb200.PRECISION_FP64))
+        nc_sub = 255
+        ntop = 3
+        mb = ctypes.c_int64()
+        L.fmmb200_shard_record_bytes(3, fmmb200.PRECISION_FP64, ctypes.byref(mb), None)
+        nc_loc = nc_sub + ntop
+        bext = torch.zeros((ntop, 6), dtype=torch.float64, device="cuda")
+        bext[:, 3:] = 1.0
+        mext = torch.zeros((ntop, mb.value), dtype=torch.uint8, device="cuda")
+        lext = torch.tensor([[0, -1]] * ntop, dtype=torch.int32, device="cuda")
+        ptr = torch.zeros(nc_loc + 1, dtype=torch.int32, device="cuda")
+        ptr[64:] = 1  # one M2L pair on cluster 63, whose source is out of range
+        src = torch.tensor([nc_loc + 5], dtype=torch.int32, device="cuda")
+        pptr = torch.zeros(nc_loc + 1, dtype=torch.int32, device="cuda")
+        E = torch.empty((5000, 3), dtype=torch.float64, device="cuda")
+        vp = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+        st = L.fmmb200_shard_evaluate(ctx.handle, 1, 0, 40, 0.5, ntop, vp(bext), vp(mext), vp(lext), 0, None, vp(ptr),
+                                      vp(src), 1, vp(pptr), None, 0, -1.0, 1.0, vp(E), vp(E))
+        assert st == fmmb200.ERR_INVALID_ARGUMENT
+
+
 def _worker(rank, world, initf, counts, out):
     sys.path.insert(0, os.path.join(ROOT, "fmm4rbgpu.jl_b200"))
     import torch
@@ -95,9 +186,10 @@ def _worker(rank, world, initf, counts, out):
     sl = slice(lo, lo + counts[rank])
     alg = fmmb200.FMMB200(n=4, N0=100, eta=0.5, precision="mixed")
     with fmmb200.Context(0) as ctx:
+        info = {}
         E, B = sharded.sharded_fields(torch.tensor(pos[sl], device="cuda"), torch.tensor(mom[sl], device="cuda"), alg,
-                                      ctx=ctx)
-        Eref, Bref = ctx.forward(pos, mom, alg)
+                                      ctx=ctx, info=info)
+        Eref, Bref = ctx.forward(pos, mom, alg, p_avg=info["pavg"])
     ok = np.array_equal(E.cpu().numpy(), Eref[sl]) and np.array_equal(B.cpu().numpy(), Bref[sl])
     out.put((rank, ok, tuple(E.shape)))
     dist.barrier()

@@ -1,8 +1,18 @@
-"""Host logic of one beam over several ranks (fmmb200.sharded) on CPU: gloo ranks that
-hold different numbers of particles (none, for one of them) exchange them, run a
-stand-in for the sharded forward and sum the shards.  The stand-in evaluates the
-oracle's FMM of the gathered beam and keeps one share of its particles per rank, so
-the exchange must return every rank exactly the oracle's fields of its own particles."""
+"""Host logic of one beam over several ranks (fmmb200.sharded) on CPU.
+
+The tree is split at level L = log2(ranks): the ranks partition its first L levels
+together (exact boxes by all-reduce, an exact distributed selection of each node's split)
+and move every particle to the rank of its level-L cluster.  Checked against the oracle's
+ClusterTree (src/cluster_tree/clusters.jl:21-70) with the same stretch:
+
+* every rank receives exactly the particles of its level-L cluster, in ascending global
+  index order, and the top levels' boxes are the oracle's, bit for bit;
+* with ranks in one process (LoopbackComm) for 2, 4 and 8 ranks, and with 2 and 4 gloo
+  processes (DistComm), ranks holding different numbers of particles (none, for one);
+* ties on the split coordinate (a lattice) are broken by the global index, as the
+  oracle's id-tie-broken selection does;
+* the gloo collectives of DistComm behave as LoopbackComm's.
+"""
 import os
 import sys
 
@@ -11,52 +21,111 @@ import pytest
 
 from conftest import ROOT
 
+sys.path.insert(0, os.path.join(ROOT, "fmm4rbgpu.jl_b200"))
 
-def _beam(n):
-    rng = np.random.default_rng(7)
+
+def _beam(n, kind="gauss", seed=7):
+    rng = np.random.default_rng(seed)
+    if kind == "lattice":
+        g = np.arange(16, dtype=float)
+        pos = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)[:n]
+        pos = pos[rng.permutation(len(pos))]
+        mom = np.zeros_like(pos)
+        mom[:, 2] = 3.0
+        return pos, mom
     pos = rng.normal(0.0, 1.0, (n, 3)) * np.array([1.0, 1.0, 0.1])
     mom = np.c_[rng.normal(0, 0.01, (n, 2)), rng.normal(200.0, 0.2, n)]
     return pos, mom
 
 
-def _stand_in(gpos, gmom, alg, rank, world, charge, lambda_):
+def _split(pos, mom, counts):
     import torch
 
-    sys.path.insert(0, ROOT)
+    out, lo = [], 0
+    for c in counts:
+        out.append(dict(pos=torch.from_numpy(pos[lo:lo + c].copy()), mom=torch.from_numpy(mom[lo:lo + c].copy())))
+        lo += c
+    return out
+
+
+def _partition(comm, slots, N0):
+    from fmmb200 import sharded
+
+    beam = sharded.prepare(comm, slots, N0)
+    top = sharded._partition_top(comm, slots, beam["N"], beam["L"], beam["stretch"])
+    sharded.redistribute(comm, slots, beam)
+    return beam, top
+
+
+def _check_against_oracle(pos, N0, beam, top, got):
+    """got: {rank: received global indices in order}."""
     import oracle
 
-    E, B, _ = oracle.fmm(gpos.numpy(), gmom.numpy(), charge, lambda_, alg.n, alg.N0, alg.eta,
-                         variant=oracle.VARIANT_GPU)
-    keep = (np.arange(len(E)) % world) == rank  # a share unrelated to who holds the particle
-    E[~keep] = 0.0
-    B[~keep] = 0.0
-    return torch.from_numpy(E), torch.from_numpy(B)
+    ref = oracle.cluster_tree(pos, N0, beam["stretch"])
+    L = beam["L"]
+    assert np.array_equal(ref["bboxes"][: (1 << L) - 1], top)
+    lo, hi = ref["parlohis"][:, 0], ref["parlohis"][:, 1]
+    for r, gids in got.items():
+        g = (1 << L) - 1 + r
+        want = np.sort(ref["parindices"][lo[g]:hi[g] + 1])
+        assert np.array_equal(gids, want), r
+        assert np.all(np.diff(gids) > 0)
+
+
+@pytest.mark.parametrize("world,counts,kind", [(2, [700, 300], "gauss"), (4, [0, 500, 523, 977], "gauss"),
+                                               (8, [400] * 8, "gauss"), (4, [1000, 1000, 1000, 1096], "lattice")])
+def test_loopback_partition_matches_the_oracle_tree(world, counts, kind):
+    from fmmb200 import sharded
+
+    pos, mom = _beam(sum(counts), kind)
+    slots = _split(pos, mom, counts)
+    N0 = 20
+    beam, top = _partition(sharded.LoopbackComm(world), slots, N0)
+    _check_against_oracle(pos, N0, beam, top, {s["rank"]: s["sub_gid"].numpy() for s in slots})
+    for s in slots:  # the received rows are the particles' own positions and momenta
+        assert np.array_equal(s["sub_pos"].numpy(), pos[s["sub_gid"].numpy()])
+        assert np.array_equal(s["sub_mom"].numpy(), mom[s["sub_gid"].numpy()])
+
+
+def test_too_many_ranks_for_the_tree_is_refused():
+    from fmmb200 import sharded
+
+    pos, mom = _beam(100)
+    with pytest.raises(ValueError):
+        sharded.prepare(sharded.LoopbackComm(8), _split(pos, mom, [13] * 7 + [9]), 20)
+    with pytest.raises(ValueError):
+        sharded.prepare(sharded.LoopbackComm(3), _split(pos, mom, [40, 30, 30]), 20)
 
 
 def _worker(rank, world, initf, counts, out):
     sys.path.insert(0, os.path.join(ROOT, "fmm4rbgpu.jl_b200"))
+    import torch
     import torch.distributed as dist
 
-    import fmmb200
     from fmmb200 import sharded
 
     dist.init_process_group("gloo", init_method=f"file://{initf}", rank=rank, world_size=world)
-    pos, mom = _beam(sum(counts))
-    lo = sum(counts[:rank])
-    mine = slice(lo, lo + counts[rank])
-    alg = fmmb200.FMMB200(n=3, N0=40, eta=0.5)
-    E, B = sharded.sharded_fields(pos[mine], mom[mine], alg, charge=-1.0, lambda_=2.0, compute=_stand_in)
-    out.put((rank, E, B))
-    dist.barrier()
-    dist.destroy_process_group()
+    try:
+        comm = sharded.DistComm()
+        pos, mom = _beam(sum(counts))
+        lo = sum(counts[:rank])
+        slot = dict(pos=torch.from_numpy(pos[lo:lo + counts[rank]].copy()),
+                    mom=torch.from_numpy(mom[lo:lo + counts[rank]].copy()))
+        beam, top = _partition(comm, [slot], 20)
+        # the collectives against their loopback meaning
+        x = torch.arange(rank + 1, dtype=torch.int64) + 10 * rank
+        gathered = [t.tolist() for t in comm.all_gather([x])[0]]
+        a2a = [t.tolist() for t in comm.all_to_all([[torch.full((q + 1,), 100 * rank + q) for q in range(world)]])[0]]
+        red = comm.all_reduce([torch.tensor([float(rank), -float(rank)])], "max")[0].tolist()
+        out.put((rank, slot["sub_gid"].numpy(), top, beam["stretch"], gathered, a2a, red))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("counts", [[700, 300], [0, 500, 523]])
-def test_ranks_get_the_oracle_fields_of_their_own_particles(tmp_path, counts):
+@pytest.mark.parametrize("counts", [[700, 300], [0, 500, 523, 977]])
+def test_gloo_ranks_partition_like_the_oracle(tmp_path, counts):
     import torch.multiprocessing as mp
-
-    sys.path.insert(0, ROOT)
-    import oracle
 
     world = len(counts)
     ctx = mp.get_context("spawn")
@@ -65,14 +134,18 @@ def test_ranks_get_the_oracle_fields_of_their_own_particles(tmp_path, counts):
     procs = [ctx.Process(target=_worker, args=(r, world, initf, counts, q)) for r in range(world)]
     for p in procs:
         p.start()
-    res = sorted((q.get(timeout=300) for _ in procs), key=lambda x: x[0])
+    try:
+        res = sorted((q.get(timeout=240) for _ in procs), key=lambda x: x[0])
+    finally:
+        for p in procs:
+            p.join(timeout=60)
     for p in procs:
-        p.join(timeout=60)
         assert p.exitcode == 0
-    pos, mom = _beam(sum(counts))
-    E, B, _ = oracle.fmm(pos, mom, -1.0, 2.0, 3, 40, 0.5, variant=oracle.VARIANT_GPU)
-    lo = 0
-    for r, Er, Br in res:
-        assert Er.shape == (counts[r], 3)
-        assert np.array_equal(Er, E[lo:lo + counts[r]]) and np.array_equal(Br, B[lo:lo + counts[r]])
-        lo += counts[r]
+    pos, _ = _beam(sum(counts))
+    beam = dict(L=world.bit_length() - 1, stretch=res[0][3])
+    _check_against_oracle(pos, 20, beam, res[0][2], {r: g for r, g, *_ in res})
+    for r, _, top, _, gathered, a2a, red in res:
+        assert np.array_equal(top, res[0][2])
+        assert gathered == [[10 * k + i for i in range(k + 1)] for k in range(world)]
+        assert a2a == [[100 * k + r] * (r + 1) for k in range(world)]
+        assert red == [float(world - 1), 0.0]
