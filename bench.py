@@ -94,8 +94,13 @@ def parse():
                     help="mixed-form M2L engine (fmmb200_set_m2l_engine)")
     ap.add_argument("--bwd-steps", type=int, default=3, help="timed fwd+bwd steps (after 2 warm-up steps)")
     ap.add_argument("--shard", action="store_true",
-                    help="one beam of --N particles split over the ranks (strong scaling, fmmb200.sharded) "
-                         "instead of one independent beam per rank")
+                    help="one beam of --N particles split over the ranks (strong scaling, fmmb200.sharded: the "
+                         "tree split at level log2(ranks), each rank holding its subtree) instead of one "
+                         "independent beam per rank")
+    ap.add_argument("--shard-emulate", default="",
+                    help="comma-separated rank counts: run the memory-sharded forward of --N particles with that "
+                         "many ranks on this one GPU (the ranks in turn, the collectives as local copies) and "
+                         "print per-rank compute time and device memory; not a multi-GPU measurement")
     return ap.parse_args()
 
 
@@ -631,11 +636,12 @@ def run_sharded(args, world, rank, local):
     pos = torch.from_numpy(pos_h[lo:hi]).to(dev)
     mom = torch.from_numpy(mom_h[lo:hi]).to(dev)
     ctx = fmmb200.Context(local)
-    ctx.set_timing(True)
+    ctx_lists = fmmb200.Context(local)
     alg = fmmb200.FMMB200(n=args.n, N0=args.N0, eta=args.eta, precision="mixed")
+    info = {}
 
     def step():
-        return sharded.sharded_fields(pos, mom, alg, ctx=ctx)
+        return sharded.sharded_fields(pos, mom, alg, ctx=ctx, ctx_lists=ctx_lists, info=info)
 
     for _ in range(args.warmup):
         step()
@@ -657,7 +663,6 @@ def run_sharded(args, world, rank, local):
     torch.cuda.synchronize(dev)
     barrier(world)
     ms = max_over_ranks(world, ev0.elapsed_time(ev1) / args.steps)
-    st = ctx.stats()
     if rank == 0:
         cfg = workload(args)
         cfg["workload"] = cfg["workload"].replace("value = mixed form, fp64 = plain path",
@@ -668,13 +673,81 @@ def run_sharded(args, world, rank, local):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "strong", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic: one seeded Gaussian bunch split over the ranks", "config": cfg,
-            "shard": {"particles_per_rank": hi - lo, "allgather_bytes_per_rank": 48 * N,
-                      "reduce_scatter_bytes_per_rank": 48 * N, "ms_m2l_rank0": st["ms_m2l"],
-                      "ms_p2p_rank0": st["ms_p2p"], "ms_tree_rank0": st["ms_tree"]},
-            "gpu_launches": int(st["kernel_launches"]) * args.steps,
+            "shard": {k: info.get(k) for k in ("particles", "halo_particles", "remote_clusters", "subtree_clusters",
+                                                  "device_bytes", "list_device_bytes", "halo_bytes",
+                                                  "remote_moment_bytes")},
             "clocks": clk.summary(),
         }), flush=True)
     ctx.close()
+    ctx_lists.close()
+
+
+def run_shard_emulate(args):
+    """The memory-sharded forward with G ranks evaluated in turn on this one GPU: per-rank
+    compute time (the rank's library calls, which return when their GPU work is done) and
+    device memory, and whether the fields equal the single-GPU forward's bit for bit."""
+    import torch
+
+    import fmmb200
+    from fmmb200 import sharded
+
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    N = args.N
+    pos_h, mom_h = generate(args, N, args.seed)
+    alg = fmmb200.FMMB200(n=args.n, N0=args.N0, eta=args.eta, precision="mixed")
+    out = {"workload": workload(args)["workload"], "N": N, "ranks": {}}
+    for G in [int(x) for x in args.shard_emulate.split(",") if x]:
+        bounds = [N * r // G for r in range(G + 1)]
+        slots = [dict(pos=torch.tensor(pos_h[bounds[r]:bounds[r + 1]], device=dev),
+                      mom=torch.tensor(mom_h[bounds[r]:bounds[r + 1]], device=dev),
+                      ctx=fmmb200.Context(0), ctx_lists=fmmb200.Context(0)) for r in range(G)]
+        comm = sharded.LoopbackComm(G)
+        res = sharded.forward_slots(comm, slots, alg)  # warm-up: allocates every rank's buffers
+        for s in slots:
+            s["ms"] = {}
+        steps = max(1, min(args.steps, 3))
+        for _ in range(steps):
+            res = sharded.forward_slots(comm, slots, alg)
+        pavg = slots[0]["info"]["pavg"]
+        per_rank = []
+        for s in slots:
+            ms = {k: v / steps for k, v in s["ms"].items()}
+            per_rank.append(dict(ms=ms, ms_total=sum(ms.values()), **{k: s["info"][k] for k in (
+                "particles", "halo_particles", "remote_clusters", "device_bytes", "list_device_bytes", "halo_bytes",
+                "remote_moment_bytes")}))
+        E = torch.cat([e for e, _ in res])
+        B = torch.cat([b for _, b in res])
+        del res
+        for s in slots:
+            s["ctx"].close()
+            s["ctx_lists"].close()
+        del slots
+        torch.cuda.empty_cache()
+        with fmmb200.Context(0) as one:
+            pos = torch.tensor(pos_h, device=dev)
+            mom = torch.tensor(mom_h, device=dev)
+            E1 = torch.empty_like(pos)
+            B1 = torch.empty_like(pos)
+            one.set_stream(torch.cuda.current_stream(dev).cuda_stream)
+            one.set_timing(True)
+            for _ in range(2):
+                one.forward_device(N, pos.data_ptr(), mom.data_ptr(), E1.data_ptr(), B1.data_ptr(), alg, p_avg=pavg)
+            torch.cuda.synchronize(dev)
+            single = one.stats()
+            same = bool(torch.equal(E, E1) and torch.equal(B, B1))
+            del pos, mom, E1, B1
+        out["ranks"][str(G)] = {"max_rank_ms": max(r["ms_total"] for r in per_rank),
+                                "max_rank_device_bytes": max(r["device_bytes"] + r["list_device_bytes"]
+                                                             for r in per_rank),
+                                "single_gpu_device_bytes": single["device_bytes"],
+                                "single_gpu_ms": single["ms_tree"] + single["ms_upward"] + single["ms_lists"]
+                                + single["ms_m2l"] + single["ms_p2p"] + single["ms_downward"],
+                                "bit_identical_to_single_gpu": same, "per_rank": per_rank}
+        del E, B
+        torch.cuda.empty_cache()
+        print(json.dumps({"shard_emulate_rows": G, **out["ranks"][str(G)]}), file=sys.stderr, flush=True)
+    print(json.dumps({"shard_emulated": out}), flush=True)
 
 
 def main():
@@ -682,6 +755,9 @@ def main():
     if args.impl == "reference":
         world, rank, _ = replicas.env_ranks()
         run_reference(args, world, rank)
+        return
+    if args.shard_emulate:
+        run_shard_emulate(args)
         return
     world, rank, local = dist_setup(args)
     try:

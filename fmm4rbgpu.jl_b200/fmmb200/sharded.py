@@ -348,6 +348,25 @@ def _check(ctx: Context, st: int):
     ctx._check(st)
 
 
+class _Clock:
+    """Host time of a rank's library calls, which return once their GPU work is done:
+    the rank's compute, without the collectives."""
+
+    def __init__(self, slot, stage):
+        self.slot, self.stage = slot, stage
+
+    def __enter__(self):
+        import time
+
+        self.t0 = time.perf_counter()
+
+    def __exit__(self, *exc):
+        import time
+
+        ms = self.slot.setdefault("ms", {})
+        ms[self.stage] = ms.get(self.stage, 0.0) + 1e3 * (time.perf_counter() - self.t0)
+
+
 def prepare(comm: Comm, slots, N0: int):
     """Sizes, global indices, p_avg (the ranks' momentum sums added in rank order) and the
     tree's shape.  Returns a dict of the beam-wide quantities; sets slot["rank"], ["gid"]."""
@@ -429,9 +448,10 @@ def forward_slots(comm: Comm, slots, alg: FMMB200, *, charge=-1.0, lambda_=1.0):
     for s in slots:
         dev = s["sub_pos"].device
         ctx = s["ctx"]
-        _check(ctx, lib.fmmb200_shard_subtree(ctx.handle, s["sub_pos"].shape[0], _vp(s["sub_pos"]),
-                                              _vp(s["sub_mom"]), alg.N0, depth, pa.ctypes.data_as(L.p_f64), alg.n,
-                                              prec))
+        with _Clock(s, "subtree"):
+            _check(ctx, lib.fmmb200_shard_subtree(ctx.handle, s["sub_pos"].shape[0], _vp(s["sub_pos"]),
+                                                  _vp(s["sub_mom"]), alg.N0, depth, pa.ctypes.data_as(L.p_f64),
+                                                  alg.n, prec))
         s["boxes"] = torch.empty((nc_sub, 6), dtype=torch.float64, device=dev)
         _check(ctx, lib.fmmb200_shard_boxes(ctx.handle, _vp(s["boxes"])))
         root = torch.zeros(1, dtype=torch.int32, device=dev)
@@ -455,8 +475,9 @@ def forward_slots(comm: Comm, slots, alg: FMMB200, *, charge=-1.0, lambda_=1.0):
             for q in range(world):
                 gb[base + (q << d): base + ((q + 1) << d)] = all_boxes[j][q][(1 << d) - 1: (2 << d) - 1]
         counts2 = (ctypes.c_int64 * 2)()
-        _check(ctxg, lib.fmmb200_shard_lists(ctxg.handle, nc, ml, _vp(gb), pa.ctypes.data_as(L.p_f64), alg.eta,
-                                             Lv, r, counts2))
+        with _Clock(s, "lists"):
+            _check(ctxg, lib.fmmb200_shard_lists(ctxg.handle, nc, ml, _vp(gb), pa.ctypes.data_as(L.p_f64), alg.eta,
+                                                 Lv, r, counts2))
         nm2l, np2p = counts2[0], counts2[1]
         mptr = torch.empty(nc + 1, dtype=torch.int32, device=dev)
         pptr = torch.empty(nc + 1, dtype=torch.int32, device=dev)
@@ -508,8 +529,9 @@ def forward_slots(comm: Comm, slots, alg: FMMB200, *, charge=-1.0, lambda_=1.0):
             moms = torch.empty(cm.numel() * mb, dtype=torch.uint8, device=dev)
             recs = torch.empty(int(cnt.sum().item()) * pb, dtype=torch.uint8, device=dev)
             clid = cl.to(torch.int32)
-            _check(ctx, lib.fmmb200_shard_pack(ctx.handle, cm.numel(), _vp(cm), _vp(moms), clid.numel(), _vp(clid),
-                                               _vp(offs_l), _vp(recs)))
+            with _Clock(s, "pack"):
+                _check(ctx, lib.fmmb200_shard_pack(ctx.handle, cm.numel(), _vp(cm), _vp(moms), clid.numel(),
+                                                   _vp(clid), _vp(offs_l), _vp(recs)))
             rows.append(torch.cat([moms, recs]))
         pay_sends.append(rows)
     pays = comm.all_to_all(pay_sends)
@@ -556,12 +578,14 @@ def forward_slots(comm: Comm, slots, alg: FMMB200, *, charge=-1.0, lambda_=1.0):
         E = torch.empty_like(s["sub_pos"])
         B = torch.empty_like(s["sub_pos"])
         max_leaf = int((leaf_hi - leaf_lo + 1).max())
-        _check(ctx, lib.fmmb200_shard_evaluate(
-            ctx.handle, Lv, r, max_leaf, float(alg.eta), next_, _vp(bext), _vp(mext), _vp(lext), nhalo,
-            _vp(halo_recs), _vp(lmptr), _vp(lmsrc), int(lmsrc.numel()), _vp(lpptr), _vp(lpsrc), int(lpsrc.numel()),
-            float(charge), float(lambda_), _vp(E), _vp(B)))
+        with _Clock(s, "evaluate"):
+            _check(ctx, lib.fmmb200_shard_evaluate(
+                ctx.handle, Lv, r, max_leaf, float(alg.eta), next_, _vp(bext), _vp(mext), _vp(lext), nhalo,
+                _vp(halo_recs), _vp(lmptr), _vp(lmsrc), int(lmsrc.numel()), _vp(lpptr), _vp(lpsrc),
+                int(lpsrc.numel()), float(charge), float(lambda_), _vp(E), _vp(B)))
         s["sub_E"], s["sub_B"] = E, B
         s["info"] = dict(rank=r, particles=int(s["sub_pos"].shape[0]), halo_particles=nhalo,
+                         halo_bytes=int(halo_recs.numel()), remote_moment_bytes=int(s["need_m"].numel() * mb),
                          remote_clusters=int(nrem), subtree_clusters=nc_sub, nm2l=int(lmsrc.numel()),
                          np2p=int(lpsrc.numel()), device_bytes=int(ctx.stats()["device_bytes"]),
                          list_device_bytes=int(s["ctx_lists"].stats()["device_bytes"]), pavg=pavg.tolist())
