@@ -56,6 +56,9 @@ struct fmmb200_ctx {
   // traversal target filter of a memory-sharded rank: only the rows of the level-trav_L
   // cluster trav_g, its descendants and its ancestors (trav_L < 0: every row)
   int trav_L = -1, trav_g = 0;
+  // largest pair counts and frontier a traversal of this context has needed (the next
+  // traversal sizes its buffers from them)
+  int64_t trav_need_p = 0, trav_need_m = 0, trav_need_f = 0;
   // the M2L target lists the M2L launchers read (a shard's compacted copy, or all)
   const char *m2l_ptr_key = "m2l_ptr";
   const char *m2l_src_key = "m2l_src";

@@ -9,6 +9,7 @@
 // outputs at offsets from a block scan, so every step is deterministic.  The
 // set of emitted pairs equals the DFS's.  Both lists are then radix-sorted by
 // (target, source) and grouped into CSR pointers over all clusters.
+#include <algorithm>
 #include <string>
 
 #include "device_util.cuh"
@@ -17,6 +18,10 @@
 namespace fmmb200 {
 
 namespace {
+
+// Device state of a traversal (long long words): frontier size, P2P and M2L pairs so
+// far, overflow flag, the largest frontier, the steps whose frontier was not empty.
+enum : int { kTsFront = 0, kTsP2P = 1, kTsM2L = 2, kTsOver = 3, kTsMaxFront = 4, kTsSteps = 5, kTsWords = 8 };
 
 constexpr int kTvThreads = 256;
 constexpr int kTvItems = 4;
@@ -72,10 +77,11 @@ __device__ __forceinline__ int classify(const ClusterGeom *__restrict__ geom, in
 
 // Counts per block: P2P pairs, M2L pairs and the child pairs of the splits (two per
 // split, fewer when the target filter drops one).
-__global__ void trav_count_kernel(const int2 *__restrict__ front, int nf, const ClusterGeom *__restrict__ geom,
-                                  const double *__restrict__ consts, double eta, int nblk, TravFilter flt,
-                                  int *__restrict__ bcount, int *__restrict__ totals) {
+__global__ void trav_count_kernel(const int2 *__restrict__ front, const long long *__restrict__ state,
+                                  const ClusterGeom *__restrict__ geom, const double *__restrict__ consts, double eta,
+                                  int nblk, TravFilter flt, int *__restrict__ bcount, int *__restrict__ totals) {
   __shared__ int s_warp[33];
+  const int nf = (int)state[kTsFront];
   const double s0 = consts[3], s1 = consts[4], s2 = consts[5];
   int c[3] = {0, 0, 0};
   int i0 = blockIdx.x * kTvTile + threadIdx.x * kTvItems;
@@ -101,11 +107,17 @@ __global__ void trav_count_kernel(const int2 *__restrict__ front, int nf, const 
   }
 }
 
-__global__ void trav_write_kernel(const int2 *__restrict__ front, int nf, const ClusterGeom *__restrict__ geom,
-                                  const double *__restrict__ consts, double eta, int nblk, TravFilter flt,
-                                  const int *__restrict__ boff, int bits, uint64_t *__restrict__ p2p,
-                                  uint64_t *__restrict__ m2l, int2 *__restrict__ next) {
+// Writes the step's pairs after the ones of the earlier steps (state) and its children as
+// the next frontier; a write past a buffer's capacity is dropped (the step's totals still
+// count it, and trav_advance_kernel raises the overflow flag).
+__global__ void trav_write_kernel(const int2 *__restrict__ front, const long long *__restrict__ state,
+                                  const ClusterGeom *__restrict__ geom, const double *__restrict__ consts, double eta,
+                                  int nblk, TravFilter flt, const int *__restrict__ boff, int bits,
+                                  uint64_t *__restrict__ p2p, long long cap_p, uint64_t *__restrict__ m2l,
+                                  long long cap_m, int2 *__restrict__ next, long long cap_f) {
   __shared__ int s_warp[33];
+  const int nf = (int)state[kTsFront];
+  const long long base_p = state[kTsP2P], base_m = state[kTsM2L];
   const double s0 = consts[3], s1 = consts[4], s2 = consts[5];
   int cat[kTvItems];
   int2 pr[kTvItems], ch1[kTvItems], ch2[kTvItems];
@@ -130,14 +142,38 @@ __global__ void trav_write_kernel(const int2 *__restrict__ front, int nf, const 
     if (cat[i] < 0) continue;
     uint64_t key = ((uint64_t)pr[i].x << bits) | (uint64_t)pr[i].y;
     if (cat[i] == kCatP2P) {
-      p2p[pos[0]++] = key;
+      const long long o = base_p + pos[0]++;
+      if (o < cap_p) p2p[o] = key;
     } else if (cat[i] == kCatM2L) {
-      m2l[pos[1]++] = key;
+      const long long o = base_m + pos[1]++;
+      if (o < cap_m) m2l[o] = key;
     } else {
-      if (trav_relevant(ch1[i].x, flt)) next[pos[2]++] = ch1[i];
-      if (trav_relevant(ch2[i].x, flt)) next[pos[2]++] = ch2[i];
+      if (trav_relevant(ch1[i].x, flt)) {
+        const int o = pos[2]++;
+        if (o < cap_f) next[o] = ch1[i];
+      }
+      if (trav_relevant(ch2[i].x, flt)) {
+        const int o = pos[2]++;
+        if (o < cap_f) next[o] = ch2[i];
+      }
     }
   }
+}
+
+// After a step: the pair counts grow by the step's totals, the frontier becomes its
+// children, and the largest needs so far are kept; a need above a capacity raises the
+// overflow flag.  The step's totals are reset for the next step.
+__global__ void trav_advance_kernel(long long *__restrict__ state, int *__restrict__ totals, long long cap_p,
+                                    long long cap_m, long long cap_f) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  state[kTsP2P] += totals[0];
+  state[kTsM2L] += totals[1];
+  const long long nf = totals[2];
+  state[kTsFront] = nf < cap_f ? nf : cap_f;
+  if (nf > state[kTsMaxFront]) state[kTsMaxFront] = nf;
+  if (nf > 0) state[kTsSteps] += 1;
+  if (state[kTsP2P] > cap_p || state[kTsM2L] > cap_m || nf > cap_f) state[kTsOver] = 1;
+  totals[0] = totals[1] = totals[2] = 0;
 }
 
 // ptr[c] = first list position with target c (lists sorted by key), src[i] = source.
@@ -309,64 +345,74 @@ int build_lists(Ctx *ctx, double eta, const double *d_consts) {
   FMM_TRY(compute_geom(ctx, d_consts));
   int bits = 1;
   while (((int64_t)1 << bits) < nc) ++bits;
-  int64_t cap_p = 64 * ctx->nleaf + 1024, cap_m = 32 * nc + 1024;
+  // Capacities: what the previous traversal of this context needed, else estimates; a
+  // traversal that outgrows one is run again with enough room (the first call of a size).
+  int64_t cap_p = std::max<int64_t>(ctx->trav_need_p, 64 * ctx->nleaf + 1024);
+  int64_t cap_m = std::max<int64_t>(ctx->trav_need_m, 32 * nc + 1024);
+  int64_t cap_f = std::max<int64_t>(ctx->trav_need_f, 4 * nc + 1024);
+  // Every step adds one level to the target or the source of a pair, so the frontier is
+  // empty after at most 2 ml + 1 steps; the loop runs that many without reading anything
+  // back, each step's work sized on the device.
+  const int max_steps = 2 * ctx->ml + 2;
   int2 *fa, *fb;
   uint64_t *p2p, *m2l;
-  int64_t front_need = 4 * nc + 1024;  // elements, the largest frontier buffer this traversal asks for
-  FMM_TRY(ctx->ensure("front_a", front_need, &fa));
-  FMM_TRY(ctx->ensure("front_b", front_need, &fb));
-  void *vp;
-  FMM_TRY(grow_keep(ctx, "p2p_keys", 0, sizeof(uint64_t) * cap_p, &vp));
-  FMM_TRY(grow_keep(ctx, "m2l_keys", 0, sizeof(uint64_t) * cap_m, &vp));
   int *bcount, *boff, *totals;
-  int *h = nullptr;
+  long long *state, *h = nullptr;
   FMM_TRY(ctx->ensure("trav_totals", 4, &totals));
-  int2 root = make_int2(0, 0);
-  FMM_CUDA_TRY(ctx, cudaMemcpyAsync(fa, &root, sizeof(int2), cudaMemcpyHostToDevice, ctx->stream));
-  int64_t nf = 1, np2p = 0, nm2l = 0;
-  int steps = 0;
+  FMM_TRY(ctx->ensure("trav_state", kTsWords, &state));
   const ClusterGeom *geom = ctx->get<ClusterGeom>("geom");
   const TravFilter flt{ctx->trav_L, ctx->trav_g};
-  while (nf > 0) {
-    const int nblk = ceil_div(nf, kTvTile);
+  int64_t np2p = 0, nm2l = 0, steps = 0;
+  for (int attempt = 0;; ++attempt) {
+    FMM_TRY(ctx->ensure("front_a", cap_f, &fa));
+    FMM_TRY(ctx->ensure("front_b", cap_f, &fb));
+    void *vp;
+    FMM_TRY(grow_keep(ctx, "p2p_keys", 0, sizeof(uint64_t) * cap_p, &vp));
+    p2p = (uint64_t *)vp;
+    FMM_TRY(grow_keep(ctx, "m2l_keys", 0, sizeof(uint64_t) * cap_m, &vp));
+    m2l = (uint64_t *)vp;
+    const int nblk = ceil_div(cap_f, kTvTile);
     FMM_TRY(ctx->ensure("trav_bcount", 3 * (int64_t)nblk, &bcount));
     FMM_TRY(ctx->ensure("trav_boff", 3 * (int64_t)nblk, &boff));
+    const long long init[kTsWords] = {1, 0, 0, 0, 1, 0, 0, 0};
+    const int2 root = make_int2(0, 0);
+    FMM_CUDA_TRY(ctx, cudaMemcpyAsync(state, init, sizeof(init), cudaMemcpyHostToDevice, ctx->stream));
+    FMM_CUDA_TRY(ctx, cudaMemcpyAsync(fa, &root, sizeof(int2), cudaMemcpyHostToDevice, ctx->stream));
     FMM_CUDA_TRY(ctx, cudaMemsetAsync(totals, 0, sizeof(int) * 4, ctx->stream));
-    trav_count_kernel<<<nblk, kTvThreads, 0, ctx->stream>>>(fa, (int)nf, geom, d_consts, eta, nblk, flt, bcount,
-                                                             totals);
-    FMM_TRY(ctx->check_launch("trav_count_kernel"));
-    FMM_TRY(exclusive_scan_i32(ctx, bcount, boff, 3 * (int64_t)nblk, nullptr));
-    FMM_TRY(ctx->pinned(sizeof(int) * 4, (void **)&h));
-    FMM_CUDA_TRY(ctx, cudaMemcpyAsync(h, totals, sizeof(int) * 3, cudaMemcpyDeviceToHost, ctx->stream));
+    for (int step = 0; step < max_steps; ++step) {
+      const int2 *cur = step % 2 == 0 ? fa : fb;
+      int2 *nxt = step % 2 == 0 ? fb : fa;
+      trav_count_kernel<<<nblk, kTvThreads, 0, ctx->stream>>>(cur, state, geom, d_consts, eta, nblk, flt, bcount,
+                                                               totals);
+      FMM_TRY(ctx->check_launch("trav_count_kernel"));
+      FMM_TRY(exclusive_scan_i32(ctx, bcount, boff, 3 * (int64_t)nblk, nullptr));
+      trav_write_kernel<<<nblk, kTvThreads, 0, ctx->stream>>>(cur, state, geom, d_consts, eta, nblk, flt, boff, bits,
+                                                               p2p, cap_p, m2l, cap_m, nxt, cap_f);
+      trav_advance_kernel<<<1, 32, 0, ctx->stream>>>(state, totals, cap_p, cap_m, cap_f);
+      FMM_TRY(ctx->check_launch("trav_write/advance kernels", 2));
+    }
+    FMM_TRY(ctx->pinned(sizeof(long long) * kTsWords, (void **)&h));
+    FMM_CUDA_TRY(ctx, cudaMemcpyAsync(h, state, sizeof(long long) * kTsWords, cudaMemcpyDeviceToHost, ctx->stream));
     FMM_TRY(ctx->sync());
-    const int64_t tp = h[0], tm = h[1], tc = h[2];  // tc: child pairs of the next frontier
-    FMM_TRY(grow_keep(ctx, "p2p_keys", sizeof(uint64_t) * np2p, sizeof(uint64_t) * (np2p + tp), &vp));
-    p2p = (uint64_t *)vp;
-    FMM_TRY(grow_keep(ctx, "m2l_keys", sizeof(uint64_t) * nm2l, sizeof(uint64_t) * (nm2l + tm), &vp));
-    m2l = (uint64_t *)vp;
-    FMM_TRY(ctx->ensure("front_b", tc + 1, &fb));  // destination: contents not needed
-    if (tc + 1 > front_need) front_need = tc + 1;
-    trav_write_kernel<<<nblk, kTvThreads, 0, ctx->stream>>>(fa, (int)nf, geom, d_consts, eta, nblk, flt, boff,
-                                                             bits, p2p + np2p, m2l + nm2l, fb);
-    FMM_TRY(ctx->check_launch("trav_write_kernel"));
-    np2p += tp;
-    nm2l += tm;
-    nf = tc;
-    std::swap(ctx->bufs["front_a"], ctx->bufs["front_b"]);
-    fa = ctx->get<int2>("front_a");
-    fb = ctx->get<int2>("front_b");
-    ++steps;
-    if (steps > 4 * 64) return ctx->fail(FMMB200_ERR_DEVICE, "traversal did not terminate");
+    np2p = h[kTsP2P];
+    nm2l = h[kTsM2L];
+    steps = h[kTsSteps] + 1;
+    if (h[kTsFront] != 0) return ctx->fail(FMMB200_ERR_DEVICE, "traversal did not terminate");
+    // keep the needs (never a capacity: repeated calls must not compound the headroom)
+    ctx->trav_need_p = std::max<int64_t>(ctx->trav_need_p, np2p);
+    ctx->trav_need_m = std::max<int64_t>(ctx->trav_need_m, nm2l);
+    ctx->trav_need_f = std::max<int64_t>(ctx->trav_need_f, h[kTsMaxFront] + 1);
+    if (!h[kTsOver]) break;
+    if (attempt >= 8) return ctx->fail(FMMB200_ERR_DEVICE, "traversal buffers did not converge");
+    // grow what overflowed; after a truncated frontier the later counts are lower bounds,
+    // so a second pass may still grow a buffer
+    if (np2p > cap_p) cap_p = std::max<int64_t>(2 * cap_p, np2p + 1024);
+    if (nm2l > cap_m) cap_m = std::max<int64_t>(2 * cap_m, nm2l + 1024);
+    if (h[kTsMaxFront] > cap_f) cap_f = std::max<int64_t>(2 * cap_f, h[kTsMaxFront] + 1024);
   }
-  // The two frontier buffers swap every step, so a step may grow either one.  Sizing both for
-  // the largest frontier of this traversal here (neither holds live data now) means the next
-  // traversal of the same tree grows neither.  The request is a need, never a capacity, so
-  // repeated calls cannot compound the allocator's headroom.
-  FMM_TRY(ctx->ensure("front_a", front_need, &fa));
-  FMM_TRY(ctx->ensure("front_b", front_need, &fb));
   ctx->nm2l = nm2l;
   ctx->np2p = np2p;
-  ctx->traversal_steps = steps;
+  ctx->traversal_steps = (int)steps;
   FMM_TRY(sort_and_group(ctx, "m2l_keys", "m2l_keys_alt", "m2l_ptr", "m2l_src", nm2l, bits));
   FMM_TRY(sort_and_group(ctx, "p2p_keys", "p2p_keys_alt", "p2p_ptr", "p2p_src", np2p, bits));
   // exact P2P work for the stats
