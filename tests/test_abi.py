@@ -192,3 +192,21 @@ def test_direct_entry_points_reject_more_targets_than_particles_without_a_list()
     assert lib.fmmb200_direct_noalloc(10, p, p, -1.0, 1.0, 11, None, p, p, None) == fmmb200.ERR_INVALID_ARGUMENT
     assert lib.fmmb200_direct_noalloc(10, p, p, -1.0, 0.0, 5, None, p, p, None) == fmmb200.ERR_INVALID_ARGUMENT
     assert lib.fmmb200_direct_device(None, 10, p, p, -1.0, 1.0, 11, None, p, p) == fmmb200.ERR_INVALID_ARGUMENT
+
+
+def test_shard_record_sizes_without_gpu():
+    """The exchange buffers of the sharded forward are sized from fmmb200_shard_record_bytes:
+    4 (n+1)^3 moment values of the precision's type, and 64 (FP64) or 80 (mixed) bytes per
+    particle record.  Bad degrees or precisions are refused."""
+    import fmmb200
+
+    lib = fmmb200.load()
+    m = ctypes.c_int64()
+    p = ctypes.c_int64()
+    assert lib.fmmb200_shard_record_bytes(4, fmmb200.PRECISION_FP64, ctypes.byref(m), ctypes.byref(p)) == fmmb200.OK
+    assert (m.value, p.value) == (4 * 125 * 8, 64)
+    assert lib.fmmb200_shard_record_bytes(5, fmmb200.PRECISION_MIXED, ctypes.byref(m), ctypes.byref(p)) == fmmb200.OK
+    assert (m.value, p.value) == (4 * 216 * 4, 80)
+    assert lib.fmmb200_shard_record_bytes(0, 0, None, None) == fmmb200.ERR_INVALID_ARGUMENT
+    assert lib.fmmb200_shard_record_bytes(4, 7, None, None) == fmmb200.ERR_INVALID_ARGUMENT
+    assert lib.fmmb200_shard_subtree(None, 10, None, None, 5, 1, None, 4, 0) == fmmb200.ERR_INVALID_ARGUMENT
