@@ -80,8 +80,7 @@ def parse():
                     help="one more reference-arm evaluation at this size, outside the timed steps, so that "
                          "the growth of the CPU cost per particle with N is visible (0: skip)")
     ap.add_argument("--skip-nsweep", action="store_true")
-    ap.add_argument("--nsweep", default="2:0.5,3:0.5,4:0.5,5:0.5,6:0.5,4:0.4,4:0.3,4:0.25,4:0.2,3:0.15,4:0.15,"
-                                        "5:0.15,3:0.1,4:0.1",
+    ap.add_argument("--nsweep", default="2:0.5,3:0.5,4:0.5,5:0.5,6:0.5,4:0.4,4:0.3,4:0.25,4:0.2",
                     help="n:eta settings of the accuracy/throughput sweep (the FMM's error against the direct sum "
                          "has a floor set by eta, from the mean momentum in its far-field kernel, so the sweep "
                          "lowers eta rather than only raising n)")
@@ -293,7 +292,7 @@ def _events_ms(stream, fn, steps, warmup):
 
 def run_nsweep(args, ctx, stream, N, pos, mom, tg, Ed, Bd):
     """Both forms at each (n, eta) of --nsweep on the benchmark beam: ms/step (1 warm-up,
-    2 timed steps each) and rel-L2 of E and B on the direct sum's targets."""
+    then 2 timed steps, 1 above a second) and rel-L2 of E and B on the direct sum's targets."""
     import torch
 
     import fmmb200
@@ -312,8 +311,11 @@ def run_nsweep(args, ctx, stream, N, pos, mom, tg, Ed, Bd):
         for prec in ("mixed", "fp64"):
             alg = fmmb200.FMMB200(n=n, N0=args.N0, eta=eta, precision=prec)
             try:
-                ms = _events_ms(stream, lambda: ctx.forward_device(N, pos.data_ptr(), mom.data_ptr(), E.data_ptr(),
-                                                                   B.data_ptr(), alg), 2, 1)
+                step = lambda: ctx.forward_device(N, pos.data_ptr(), mom.data_ptr(), E.data_ptr(),  # noqa: E731
+                                                  B.data_ptr(), alg)
+                ms = _events_ms(stream, step, 1, 1)
+                if ms < 1000.0:  # a second timed step where it is cheap
+                    ms = _events_ms(stream, step, 2, 0)
             except fmmb200.FMMB200Error as e:  # e.g. out of device memory at the largest n
                 row[prec] = {"error": str(e)}
                 continue
