@@ -397,15 +397,11 @@ __global__ void __launch_bounds__(BShape<NDEG>::BT)
         gc[e] += v;
       }
     }
-    // geometry: e_d[a] += sum_q X[q][a] * (T^{(d)} Y)[q][a] for d = x, y, z
-    for (int d = 0; d < 3; ++d) {
-      const double(*Wx)[M] = d == 0 ? D[ch][0] : L[ch][0];
-      const double(*Wy)[M] = d == 1 ? D[ch][1] : L[ch][1];
-      const double(*Wz)[M] = d == 2 ? D[ch][2] : L[ch][2];
-      stage_x(Wx, s_y);
-      __syncthreads();
-      stage_y(Wy);
-      __syncthreads();
+    // geometry: e_d[a] += sum_q X[q][a] * (T^{(d)} Y)[q][a] for d = x, y, z.  Axes z and y
+    // share the x stage Lx Y, and for M2M^T the propagation above already left Lx Y in s_t1
+    // and Ly Lx Y in s_t2 (the z axis needs exactly those), so the three contractions take
+    // 6 stages after M2M^T's propagation and 8 after L2L^T's instead of 9.
+    auto stage_ze = [&](int d, const double(*Wz)[M]) {
 #pragma unroll
       for (int r = 0; r < NPT; ++r) {
         const int a = tid + r * BT;
@@ -422,7 +418,24 @@ __global__ void __launch_bounds__(BShape<NDEG>::BT)
           eacc[r][d] += sum;
         }
       }
+    };
+    if (MODE == 0) {
+      stage_x(L[ch][0], s_y);
+      __syncthreads();
+      stage_y(L[ch][1]);
+      __syncthreads();
     }
+    stage_ze(2, D[ch][2]);  // z: Dz Ly Lx Y
+    __syncthreads();
+    stage_y(D[ch][1]);      // y: Lz Dy Lx Y, from the Lx Y still in s_t1
+    __syncthreads();
+    stage_ze(1, L[ch][2]);
+    __syncthreads();
+    stage_x(D[ch][0], s_y);  // x: Lz Ly Dx Y
+    __syncthreads();
+    stage_y(L[ch][1]);
+    __syncthreads();
+    stage_ze(0, L[ch][2]);
     // G_d[i] = sum over the nodes with index i on axis d
 #pragma unroll
     for (int r = 0; r < NPT; ++r) {

@@ -59,6 +59,7 @@ struct fmmb200_ctx {
   // largest pair counts and frontier a traversal of this context has needed (the next
   // traversal sizes its buffers from them)
   int64_t trav_need_p = 0, trav_need_m = 0, trav_need_f = 0;
+  double trav_key[4] = {-1, -1, -1, -1};  // (clusters, eta, filter level, filter cluster) of those needs
   // the M2L target lists the M2L launchers read (a shard's compacted copy, or all)
   const char *m2l_ptr_key = "m2l_ptr";
   const char *m2l_src_key = "m2l_src";

@@ -10,6 +10,7 @@
 // set of emitted pairs equals the DFS's.  Both lists are then radix-sorted by
 // (target, source) and grouped into CSR pointers over all clusters.
 #include <algorithm>
+#include <cstring>
 #include <string>
 
 #include "device_util.cuh"
@@ -75,34 +76,71 @@ __device__ __forceinline__ int classify(const ClusterGeom *__restrict__ geom, in
   return kCatSplit;
 }
 
-// Counts per block: P2P pairs, M2L pairs and the child pairs of the splits (two per
-// split, fewer when the target filter drops one).
+// Counts per tile of the frontier: P2P pairs, M2L pairs and the child pairs of the
+// splits (two per split, fewer when the target filter drops one).  The grid is fixed and
+// strides over the tiles that the frontier (state, on the device) occupies.
 __global__ void trav_count_kernel(const int2 *__restrict__ front, const long long *__restrict__ state,
                                   const ClusterGeom *__restrict__ geom, const double *__restrict__ consts, double eta,
                                   int nblk, TravFilter flt, int *__restrict__ bcount, int *__restrict__ totals) {
   __shared__ int s_warp[33];
   const int nf = (int)state[kTsFront];
+  const int ntile = (nf + kTvTile - 1) / kTvTile;
   const double s0 = consts[3], s1 = consts[4], s2 = consts[5];
-  int c[3] = {0, 0, 0};
-  int i0 = blockIdx.x * kTvTile + threadIdx.x * kTvItems;
-  for (int i = 0; i < kTvItems; ++i) {
-    int q = i0 + i;
-    if (q < nf) {
-      int2 p = front[q];
-      int a, b, cc, d;
-      const int cat = classify(geom, p.x, p.y, s0, s1, s2, eta, &a, &b, &cc, &d);
-      if (cat == kCatSplit)
-        c[2] += (int)trav_relevant(a, flt) + (int)trav_relevant(cc, flt);
-      else
-        c[cat]++;
+  for (int tile = blockIdx.x; tile < ntile; tile += gridDim.x) {
+    int c[3] = {0, 0, 0};
+    const int i0 = tile * kTvTile + threadIdx.x * kTvItems;
+    for (int i = 0; i < kTvItems; ++i) {
+      const int q = i0 + i;
+      if (q < nf) {
+        const int2 p = front[q];
+        int a, b, cc, d;
+        const int cat = classify(geom, p.x, p.y, s0, s1, s2, eta, &a, &b, &cc, &d);
+        if (cat == kCatSplit)
+          c[2] += (int)trav_relevant(a, flt) + (int)trav_relevant(cc, flt);
+        else
+          c[cat]++;
+      }
+    }
+    for (int k = 0; k < 3; ++k) {
+      int tot;
+      block_excl_scan(c[k], s_warp, &tot);
+      if (threadIdx.x == 0) {
+        bcount[k * nblk + tile] = tot;
+        if (tot) atomicAdd(&totals[k], tot);
+      }
+      __syncthreads();
     }
   }
+}
+
+// Exclusive scan, per category, of the counts of the tiles the frontier occupies (one
+// block; boff[k * nblk] = 0).
+constexpr int kTileScanItems = 16;
+__global__ void __launch_bounds__(1024) tile_scan_kernel(const int *__restrict__ bcount, int nblk,
+                                                         const long long *__restrict__ state, int *__restrict__ boff) {
+  __shared__ int s_warp[33];
+  const int ntile = (int)((state[kTsFront] + kTvTile - 1) / kTvTile);
   for (int k = 0; k < 3; ++k) {
-    int tot;
-    block_excl_scan(c[k], s_warp, &tot);
-    if (threadIdx.x == 0) {
-      bcount[k * nblk + blockIdx.x] = tot;
-      if (tot) atomicAdd(&totals[k], tot);
+    const int *in = bcount + (int64_t)k * nblk;
+    int *out = boff + (int64_t)k * nblk;
+    int carry = 0;
+    for (int c0 = 0; c0 < ntile; c0 += 1024 * kTileScanItems) {
+      const int i0 = c0 + threadIdx.x * kTileScanItems;
+      int v[kTileScanItems], sum = 0;
+#pragma unroll
+      for (int j = 0; j < kTileScanItems; ++j) {
+        v[j] = i0 + j < ntile ? in[i0 + j] : 0;
+        sum += v[j];
+      }
+      int chunk;
+      int run = carry + block_excl_scan(sum, s_warp, &chunk);
+#pragma unroll
+      for (int j = 0; j < kTileScanItems; ++j) {
+        if (i0 + j < ntile) out[i0 + j] = run;
+        run += v[j];
+      }
+      carry += chunk;
+      __syncthreads();
     }
   }
 }
@@ -117,44 +155,49 @@ __global__ void trav_write_kernel(const int2 *__restrict__ front, const long lon
                                   long long cap_m, int2 *__restrict__ next, long long cap_f) {
   __shared__ int s_warp[33];
   const int nf = (int)state[kTsFront];
+  const int ntile = (nf + kTvTile - 1) / kTvTile;
   const long long base_p = state[kTsP2P], base_m = state[kTsM2L];
   const double s0 = consts[3], s1 = consts[4], s2 = consts[5];
-  int cat[kTvItems];
-  int2 pr[kTvItems], ch1[kTvItems], ch2[kTvItems];
-  int c[3] = {0, 0, 0};
-  int i0 = blockIdx.x * kTvTile + threadIdx.x * kTvItems;
-  for (int i = 0; i < kTvItems; ++i) {
-    int q = i0 + i;
-    cat[i] = -1;
-    if (q < nf) {
-      pr[i] = front[q];
-      cat[i] = classify(geom, pr[i].x, pr[i].y, s0, s1, s2, eta, &ch1[i].x, &ch1[i].y, &ch2[i].x, &ch2[i].y);
-      if (cat[i] == kCatSplit)
-        c[2] += (int)trav_relevant(ch1[i].x, flt) + (int)trav_relevant(ch2[i].x, flt);
-      else
-        c[cat[i]]++;
-    }
-  }
-  int pos[3];
-  for (int k = 0; k < 3; ++k)
-    pos[k] = block_excl_scan(c[k], s_warp, nullptr) + boff[k * nblk + blockIdx.x] - boff[k * nblk];
-  for (int i = 0; i < kTvItems; ++i) {
-    if (cat[i] < 0) continue;
-    uint64_t key = ((uint64_t)pr[i].x << bits) | (uint64_t)pr[i].y;
-    if (cat[i] == kCatP2P) {
-      const long long o = base_p + pos[0]++;
-      if (o < cap_p) p2p[o] = key;
-    } else if (cat[i] == kCatM2L) {
-      const long long o = base_m + pos[1]++;
-      if (o < cap_m) m2l[o] = key;
-    } else {
-      if (trav_relevant(ch1[i].x, flt)) {
-        const int o = pos[2]++;
-        if (o < cap_f) next[o] = ch1[i];
+  for (int tile = blockIdx.x; tile < ntile; tile += gridDim.x) {
+    int cat[kTvItems];
+    int2 pr[kTvItems], ch1[kTvItems], ch2[kTvItems];
+    int c[3] = {0, 0, 0};
+    const int i0 = tile * kTvTile + threadIdx.x * kTvItems;
+    for (int i = 0; i < kTvItems; ++i) {
+      const int q = i0 + i;
+      cat[i] = -1;
+      if (q < nf) {
+        pr[i] = front[q];
+        cat[i] = classify(geom, pr[i].x, pr[i].y, s0, s1, s2, eta, &ch1[i].x, &ch1[i].y, &ch2[i].x, &ch2[i].y);
+        if (cat[i] == kCatSplit)
+          c[2] += (int)trav_relevant(ch1[i].x, flt) + (int)trav_relevant(ch2[i].x, flt);
+        else
+          c[cat[i]]++;
       }
-      if (trav_relevant(ch2[i].x, flt)) {
-        const int o = pos[2]++;
-        if (o < cap_f) next[o] = ch2[i];
+    }
+    int pos[3];
+    for (int k = 0; k < 3; ++k) {
+      pos[k] = block_excl_scan(c[k], s_warp, nullptr) + boff[k * nblk + tile];
+      __syncthreads();
+    }
+    for (int i = 0; i < kTvItems; ++i) {
+      if (cat[i] < 0) continue;
+      uint64_t key = ((uint64_t)pr[i].x << bits) | (uint64_t)pr[i].y;
+      if (cat[i] == kCatP2P) {
+        const long long o = base_p + pos[0]++;
+        if (o < cap_p) p2p[o] = key;
+      } else if (cat[i] == kCatM2L) {
+        const long long o = base_m + pos[1]++;
+        if (o < cap_m) m2l[o] = key;
+      } else {
+        if (trav_relevant(ch1[i].x, flt)) {
+          const int o = pos[2]++;
+          if (o < cap_f) next[o] = ch1[i];
+        }
+        if (trav_relevant(ch2[i].x, flt)) {
+          const int o = pos[2]++;
+          if (o < cap_f) next[o] = ch2[i];
+        }
       }
     }
   }
@@ -217,6 +260,28 @@ __global__ void p2p_work_kernel(const uint64_t *__restrict__ keys, int64_t n, in
   if (threadIdx.x == 0 && s) atomicAdd(out, s);
 }
 
+// Counts the pairs (t,s) of a sorted list whose transpose (s,t) is missing.
+__global__ void transpose_missing_kernel(const uint64_t *__restrict__ keys, int64_t n, int bits,
+                                         unsigned long long *__restrict__ missing) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  int miss = 0;
+  if (i < n) {
+    const uint64_t k = keys[i], mask = ((uint64_t)1 << bits) - 1;
+    const uint64_t want = ((k & mask) << bits) | (k >> bits);
+    int64_t lo = 0, hi = n;
+    while (lo < hi) {
+      const int64_t mid = (lo + hi) >> 1;
+      if (keys[mid] < want)
+        lo = mid + 1;
+      else
+        hi = mid;
+    }
+    miss = !(lo < n && keys[lo] == want);
+  }
+  const unsigned long long w = warp_sum((unsigned long long)miss);
+  if ((threadIdx.x & 31) == 0 && w) atomicAdd(missing, w);
+}
+
 // Union of a sorted pair list and its transpose: entry (t,s) with bit 61 if
 // (t,s) is in the list and bit 62 if (s,t) is.
 __global__ void union_fill_kernel(const uint64_t *__restrict__ keys, int64_t n, int bits, uint64_t *__restrict__ out) {
@@ -262,8 +327,40 @@ int sort_and_group(Ctx *ctx, const char *keys_name, const char *alt_name, const 
   return ctx->check_launch("sort_and_group", n > 0 ? 2 : 1);
 }
 
-int build_union(Ctx *ctx, const char *keys_name, int64_t n, const char *prefix) {
+int build_union(Ctx *ctx, const char *keys_name, int64_t n, const char *prefix, const char *list_prefix) {
   const int bits = ctx->list_bits;
+  const std::string kn = std::string(prefix) + "_keys", fn = std::string(prefix) + "_flag";
+  const std::string pn = std::string(prefix) + "_ptr", sn = std::string(prefix) + "_src";
+  // A symmetric list (the usual case: the traversal's rules are symmetric except for ties of
+  // the diameters) is its own union, every pair in both roles: the same CSR, flags 3.
+  if (n > 0) {
+    unsigned long long *d_miss, *h_miss;
+    FMM_TRY(ctx->ensure("union_missing", 1, &d_miss));
+    FMM_CUDA_TRY(ctx, cudaMemsetAsync(d_miss, 0, sizeof(unsigned long long), ctx->stream));
+    transpose_missing_kernel<<<ceil_div(n, 256), 256, 0, ctx->stream>>>(ctx->get<uint64_t>(keys_name), n, bits, d_miss);
+    FMM_TRY(ctx->check_launch("transpose_missing_kernel"));
+    FMM_TRY(ctx->pinned(sizeof(unsigned long long), (void **)&h_miss));
+    FMM_CUDA_TRY(ctx, cudaMemcpyAsync(h_miss, d_miss, sizeof(unsigned long long), cudaMemcpyDeviceToHost, ctx->stream));
+    FMM_TRY(ctx->sync());
+    if (*h_miss == 0) {
+      uint64_t *uk;
+      uint8_t *uf;
+      int *ptr, *src;
+      FMM_TRY(ctx->ensure(kn.c_str(), n, &uk));
+      FMM_TRY(ctx->ensure(fn.c_str(), n, &uf));
+      FMM_TRY(ctx->ensure(pn.c_str(), ctx->nc + 1, &ptr));
+      FMM_TRY(ctx->ensure(sn.c_str(), n, &src));
+      const std::string lp = std::string(list_prefix) + "_ptr", ls = std::string(list_prefix) + "_src";
+      FMM_CUDA_TRY(ctx, cudaMemcpyAsync(uk, ctx->get<uint64_t>(keys_name), sizeof(uint64_t) * n,
+                                        cudaMemcpyDeviceToDevice, ctx->stream));
+      FMM_CUDA_TRY(ctx, cudaMemsetAsync(uf, 3, n, ctx->stream));
+      FMM_CUDA_TRY(ctx, cudaMemcpyAsync(ptr, ctx->get<int>(lp.c_str()), sizeof(int) * (ctx->nc + 1),
+                                        cudaMemcpyDeviceToDevice, ctx->stream));
+      FMM_CUDA_TRY(ctx, cudaMemcpyAsync(src, ctx->get<int>(ls.c_str()), sizeof(int) * n, cudaMemcpyDeviceToDevice,
+                                        ctx->stream));
+      return FMMB200_OK;
+    }
+  }
   const int64_t n2 = 2 * n;
   uint64_t *u, *ua;
   int *head, *pos;
@@ -283,8 +380,6 @@ int build_union(Ctx *ctx, const char *keys_name, int64_t n, const char *prefix) 
     FMM_TRY(ctx->check_launch("union_head_kernel"));
     FMM_TRY(exclusive_scan_i32(ctx, head, pos, n2, &nu));
   }
-  const std::string kn = std::string(prefix) + "_keys", fn = std::string(prefix) + "_flag";
-  const std::string pn = std::string(prefix) + "_ptr", sn = std::string(prefix) + "_src";
   uint64_t *uk;
   uint8_t *uf;
   int *ptr, *src;
@@ -335,8 +430,8 @@ int grow_keep(Ctx *ctx, const char *name, size_t used, size_t need, void **out) 
 }
 
 int build_union_lists(Ctx *ctx) {
-  FMM_TRY(build_union(ctx, "m2l_keys", ctx->nm2l, "m2lu"));
-  FMM_TRY(build_union(ctx, "p2p_keys", ctx->np2p, "p2pu"));
+  FMM_TRY(build_union(ctx, "m2l_keys", ctx->nm2l, "m2lu", "m2l"));
+  FMM_TRY(build_union(ctx, "p2p_keys", ctx->np2p, "p2pu", "p2p"));
   return FMMB200_OK;
 }
 
@@ -345,8 +440,15 @@ int build_lists(Ctx *ctx, double eta, const double *d_consts) {
   FMM_TRY(compute_geom(ctx, d_consts));
   int bits = 1;
   while (((int64_t)1 << bits) < nc) ++bits;
-  // Capacities: what the previous traversal of this context needed, else estimates; a
-  // traversal that outgrows one is run again with enough room (the first call of a size).
+  // Capacities: what the previous traversal of the same tree shape, eta and filter needed,
+  // else estimates; a traversal that outgrows one is run again with enough room (the first
+  // call of a configuration).  The frontier capacity also sizes every step's grid, so the
+  // needs of another configuration are not carried over.
+  const double key[4] = {(double)nc, eta, (double)ctx->trav_L, (double)ctx->trav_g};
+  if (std::memcmp(key, ctx->trav_key, sizeof(key)) != 0) {
+    std::memcpy(ctx->trav_key, key, sizeof(key));
+    ctx->trav_need_p = ctx->trav_need_m = ctx->trav_need_f = 0;
+  }
   int64_t cap_p = std::max<int64_t>(ctx->trav_need_p, 64 * ctx->nleaf + 1024);
   int64_t cap_m = std::max<int64_t>(ctx->trav_need_m, 32 * nc + 1024);
   int64_t cap_f = std::max<int64_t>(ctx->trav_need_f, 4 * nc + 1024);
@@ -371,7 +473,8 @@ int build_lists(Ctx *ctx, double eta, const double *d_consts) {
     p2p = (uint64_t *)vp;
     FMM_TRY(grow_keep(ctx, "m2l_keys", 0, sizeof(uint64_t) * cap_m, &vp));
     m2l = (uint64_t *)vp;
-    const int nblk = ceil_div(cap_f, kTvTile);
+    const int nblk = ceil_div(cap_f, kTvTile);             // tiles the frontier can occupy
+    const int grid = nblk < 148 * 8 ? nblk : 148 * 8;       // blocks, striding over the tiles in use
     FMM_TRY(ctx->ensure("trav_bcount", 3 * (int64_t)nblk, &bcount));
     FMM_TRY(ctx->ensure("trav_boff", 3 * (int64_t)nblk, &boff));
     const long long init[kTsWords] = {1, 0, 0, 0, 1, 0, 0, 0};
@@ -382,14 +485,13 @@ int build_lists(Ctx *ctx, double eta, const double *d_consts) {
     for (int step = 0; step < max_steps; ++step) {
       const int2 *cur = step % 2 == 0 ? fa : fb;
       int2 *nxt = step % 2 == 0 ? fb : fa;
-      trav_count_kernel<<<nblk, kTvThreads, 0, ctx->stream>>>(cur, state, geom, d_consts, eta, nblk, flt, bcount,
+      trav_count_kernel<<<grid, kTvThreads, 0, ctx->stream>>>(cur, state, geom, d_consts, eta, nblk, flt, bcount,
                                                                totals);
-      FMM_TRY(ctx->check_launch("trav_count_kernel"));
-      FMM_TRY(exclusive_scan_i32(ctx, bcount, boff, 3 * (int64_t)nblk, nullptr));
-      trav_write_kernel<<<nblk, kTvThreads, 0, ctx->stream>>>(cur, state, geom, d_consts, eta, nblk, flt, boff, bits,
+      tile_scan_kernel<<<1, 1024, 0, ctx->stream>>>(bcount, nblk, state, boff);
+      trav_write_kernel<<<grid, kTvThreads, 0, ctx->stream>>>(cur, state, geom, d_consts, eta, nblk, flt, boff, bits,
                                                                p2p, cap_p, m2l, cap_m, nxt, cap_f);
       trav_advance_kernel<<<1, 32, 0, ctx->stream>>>(state, totals, cap_p, cap_m, cap_f);
-      FMM_TRY(ctx->check_launch("trav_write/advance kernels", 2));
+      FMM_TRY(ctx->check_launch("trav_count/scan/write/advance kernels", 4));
     }
     FMM_TRY(ctx->pinned(sizeof(long long) * kTsWords, (void **)&h));
     FMM_CUDA_TRY(ctx, cudaMemcpyAsync(h, state, sizeof(long long) * kTsWords, cudaMemcpyDeviceToHost, ctx->stream));
@@ -408,7 +510,7 @@ int build_lists(Ctx *ctx, double eta, const double *d_consts) {
     // so a second pass may still grow a buffer
     if (np2p > cap_p) cap_p = std::max<int64_t>(2 * cap_p, np2p + 1024);
     if (nm2l > cap_m) cap_m = std::max<int64_t>(2 * cap_m, nm2l + 1024);
-    if (h[kTsMaxFront] > cap_f) cap_f = std::max<int64_t>(2 * cap_f, h[kTsMaxFront] + 1024);
+    if (h[kTsMaxFront] > cap_f) cap_f = std::max<int64_t>(2 * cap_f, 2 * h[kTsMaxFront]);  // a lower bound
   }
   ctx->nm2l = nm2l;
   ctx->np2p = np2p;
