@@ -545,6 +545,20 @@ def run_ours(args, world, rank, local):
             "flops_per_launch": m2l_flops, "ms_per_launch": st["ms_m2l"],
             "fp64": {"kernel": f"m2l_kernel<{args.n}> (fp64)", "achieved": ach64, "peak": p64.value,
                      "frac": ach64 / p64.value if p64.value else None, "ms_per_launch": st64["ms_m2l"]}}
+    # The FP32 pipe executes one FMA-class operation per lane per cycle, packed or not, so an
+    # operation count per evaluation turns the kernel time into the pipe's occupancy:
+    # M2L 15 per evaluation (3 denominator, 2 s^3, 10 factored sums), P2P 31 for tiles near
+    # the target leaf (9 for R from hi/lo parts, 3 R.R, 3 u.R, 1 d, 2 s^3, 3 K, 3 E, 6 B) and
+    # 25 for the far ones (R from the hi parts alone); the peak is the measured FMA rate / 2.
+    pipe = p32.value * 1e12 / 2.0
+    if st["ms_m2l"] > 0 and pipe > 0:
+        roof["fp32_pipe_occupancy"] = 15.0 * st["m2l_kernel_evals"] / (st["ms_m2l"] * 1e-3) / pipe
+    if st["ms_p2p"] > 0:
+        ach_p = 41.0 * st["p2p_kernel_evals"] / (st["ms_p2p"] * 1e-3) / 1e12
+        roof["p2p"] = {"kernel": "p2p_x2_kernel (mixed)", "achieved": ach_p, "peak": p32.value, "unit": "TFLOP/s",
+                       "frac": ach_p / p32.value if p32.value else None, "ms_per_launch": st["ms_p2p"],
+                       "fp32_pipe_occupancy_if_all_near": 31.0 * st["p2p_kernel_evals"] / (st["ms_p2p"] * 1e-3)
+                       / pipe if pipe > 0 else None}
 
     # end to end through the host-pointer C-ABI (pinned host buffers)
     e2e = None
