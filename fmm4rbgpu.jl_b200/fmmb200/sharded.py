@@ -428,9 +428,17 @@ def forward_slots(comm: Comm, slots, alg: FMMB200, *, charge=-1.0, lambda_=1.0):
     """The sharded forward of every slot held here.  slots[i]: dict with "pos", "mom"
     ((n, 3) float64 device tensors of that rank's particles), "ctx" and "ctx_lists"
     (Contexts on that rank's GPU).  Returns per slot (E, B) of its particles, and sets
-    slot["info"] (sizes and device bytes of the rank)."""
+    slot["info"] (sizes and device bytes of the rank).
+
+    Both contexts of every slot are set to run on torch's current stream of its device:
+    the library's steps read tensors that torch ops have just written, and on the same
+    stream they run after those ops (each step returns once its own work is done)."""
     import torch
 
+    for s in slots:
+        st = torch.cuda.current_stream(s["pos"].device).cuda_stream
+        s["ctx"].set_stream(st)
+        s["ctx_lists"].set_stream(st)
     beam = prepare(comm, slots, alg.N0)
     world, Lv, N, ml = beam["world"], beam["L"], beam["N"], beam["ml"]
     counts, offs, pavg = beam["counts"], beam["offs"], beam["pavg"]

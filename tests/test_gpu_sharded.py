@@ -9,7 +9,9 @@
   ranks in one process (LoopbackComm, the ranks evaluated in turn) give the single-GPU
   forward's fields with the same p_avg bit for bit, FP64 and mixed, Gaussian bunch and
   beamlets, eta below and above 1/2, ranks with different numbers of particles (none, for
-  one); each rank holds far less device memory than the single-GPU forward.
+  one), on the third of three calls with the same contexts; each rank holds far less device
+  memory than the single-GPU forward.  At N = 2^22 with 2 ranks the same holds for the
+  benchmark's distribution and parameters.
 * Two processes on the one GPU joined by gloo (fmmb200.sharded.sharded_fields): each gets
   the single-GPU fields of its own particles bit for bit.  Their kernels never wait on each
   other; the exchange runs on host copies.
@@ -116,7 +118,9 @@ def test_memory_sharded_forward_equals_the_single_gpu_forward(gpu_ctx, world, co
     alg = fmmb200.FMMB200(n=n, N0=N0, eta=eta, precision=precision)
     slots = _slots(pos, mom, counts)
     try:
-        out = sharded.forward_slots(sharded.LoopbackComm(world), slots, alg, charge=-1.0, lambda_=2.0)
+        # several calls on the same contexts: buffers grown by one call are reused by the next
+        for _ in range(3):
+            out = sharded.forward_slots(sharded.LoopbackComm(world), slots, alg, charge=-1.0, lambda_=2.0)
         pavg = slots[0]["info"]["pavg"]
         assert all(s["info"]["pavg"] == pavg for s in slots)
         with fmmb200.Context(0) as one:
@@ -131,6 +135,33 @@ def test_memory_sharded_forward_equals_the_single_gpu_forward(gpu_ctx, world, co
         for s in slots:
             s["ctx"].close()
             s["ctx_lists"].close()
+
+
+def test_memory_sharded_forward_at_2_22_two_ranks(gpu_ctx):
+    """The benchmark's bunch and parameters (n = 4, N0 = 125, eta = 0.5, mixed) at N = 2^22 over
+    two ranks, the case with the largest per-rank traversal, on the third call."""
+    import fmmb200
+    from fmmb200 import beams, sharded
+
+    N = 2**22
+    pos, mom = beams.gaussian_bunch(N, seed=0)
+    alg = fmmb200.FMMB200(n=4, N0=125, eta=0.5, precision="mixed")
+    slots = _slots(pos, mom, [N // 2, N - N // 2])
+    try:
+        for _ in range(3):
+            out = sharded.forward_slots(sharded.LoopbackComm(2), slots, alg)
+        pavg = slots[0]["info"]["pavg"]
+        halo = [s["info"]["halo_particles"] for s in slots]
+        E = np.concatenate([e.cpu().numpy() for e, _ in out])
+        del out
+    finally:
+        for s in slots:
+            s["ctx"].close()
+            s["ctx_lists"].close()
+    with fmmb200.Context(0) as one:
+        E1, _ = one.forward(pos, mom, alg, p_avg=pavg)
+    assert np.array_equal(E, E1)
+    assert max(halo) < 1.5 * min(halo)  # the two sides of the split plane need similar halos
 
 
 def test_memory_sharded_lists_are_checked(gpu_ctx):
