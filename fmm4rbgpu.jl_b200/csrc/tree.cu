@@ -365,9 +365,9 @@ __device__ __forceinline__ int sub_of(int lo0, int hi0, int depth, int p, int *l
   return s;
 }
 
-// Three CTAs per SM (shared memory allows three; the unbounded build's 126 registers
-// allowed two): at most 80 registers, with a 16-byte spill.
-__global__ void __launch_bounds__(kStThreads, 3)
+// 126 registers, two CTAs per SM.  A bound of three CTAs per SM (80 registers, a 16-byte
+// spill) made the tree stage 0.2 ms slower at N = 2^24.
+__global__ void __launch_bounds__(kStThreads)
     subtree_kernel(int L0, int ml, int N, const double *__restrict__ pos, const uint32_t *__restrict__ lists,
                    int *__restrict__ lohi, const double *__restrict__ consts, double *__restrict__ bbox,
                    int *__restrict__ argext, uint32_t *__restrict__ perm, int *__restrict__ lid,
