@@ -23,6 +23,8 @@ from . import _lib as L
 from ._lib import FMMB200Error
 
 R_E = 2.8179403699772166e-15
+# cudaStreamLegacy ((cudaStream_t)0x1): the legacy default stream as an explicit handle
+CUDA_STREAM_LEGACY = 1
 
 
 def _f64(a, shape=None):
@@ -140,7 +142,12 @@ class Context:
 
     # ---------------------------------------------------------------- settings
     def set_stream(self, stream_ptr: int | None):
-        self._check(self._lib.fmmb200_set_stream(self._h, ctypes.c_void_p(stream_ptr or 0)))
+        """Run on a cudaStream_t handle (``torch.cuda.Stream.cuda_stream``); None: the
+        context's own stream.  The handle 0, torch's default stream, is the legacy default
+        stream and is passed as cudaStreamLegacy: the library reads a NULL handle as its own
+        stream, which is non-blocking and would not be ordered after torch's work."""
+        handle = None if stream_ptr is None else (CUDA_STREAM_LEGACY if stream_ptr == 0 else stream_ptr)
+        self._check(self._lib.fmmb200_set_stream(self._h, ctypes.c_void_p(handle)))
 
     def set_timing(self, enable: bool):
         self._check(self._lib.fmmb200_set_timing(self._h, int(bool(enable))))

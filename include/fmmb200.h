@@ -71,7 +71,10 @@ int fmmb200_version(void);
 int fmmb200_create(fmmb200_ctx **ctx, int device);
 int fmmb200_destroy(fmmb200_ctx *ctx);
 const char *fmmb200_last_error(const fmmb200_ctx *ctx);
-/* Run on a caller-provided cudaStream_t (NULL restores the context's own stream). */
+/* Run on a caller-provided cudaStream_t (NULL restores the context's own stream, a
+ * cudaStreamNonBlocking stream that is not ordered after work on the legacy default
+ * stream).  To run after work on the legacy default stream (torch's default stream,
+ * whose handle reads as 0), pass cudaStreamLegacy. */
 int fmmb200_set_stream(fmmb200_ctx *ctx, void *stream);
 /* Record per-stage CUDA events (stats ms_*); off by default. */
 int fmmb200_set_timing(fmmb200_ctx *ctx, int enable);

@@ -210,3 +210,27 @@ def test_shard_record_sizes_without_gpu():
     assert lib.fmmb200_shard_record_bytes(0, 0, None, None) == fmmb200.ERR_INVALID_ARGUMENT
     assert lib.fmmb200_shard_record_bytes(4, 7, None, None) == fmmb200.ERR_INVALID_ARGUMENT
     assert lib.fmmb200_shard_subtree(None, 10, None, None, 5, 1, None, 4, 0) == fmmb200.ERR_INVALID_ARGUMENT
+
+
+def test_set_stream_passes_the_legacy_default_stream_explicitly():
+    """torch's default stream has the handle 0, and fmmb200_set_stream reads a NULL handle as
+    the context's own (non-blocking) stream, which is not ordered after torch's work: the
+    Python wrapper passes 0 as cudaStreamLegacy (0x1), other handles as given, and None as
+    NULL (the own stream)."""
+    import fmmb200
+    from fmmb200 import api
+
+    got = []
+
+    class FakeLib:
+        def fmmb200_set_stream(self, h, stream):
+            got.append(stream.value)
+            return fmmb200.OK
+
+    ctx = api.Context.__new__(api.Context)
+    ctx._lib, ctx._h = FakeLib(), ctypes.c_void_p(1234)
+    for handle in (0, None, 0x7F00DEAD):
+        ctx.set_stream(handle)
+    ctx._h = None  # nothing to destroy
+    assert got == [api.CUDA_STREAM_LEGACY, None, 0x7F00DEAD]
+    assert api.CUDA_STREAM_LEGACY == 1

@@ -137,13 +137,14 @@ def test_memory_sharded_forward_equals_the_single_gpu_forward(gpu_ctx, world, co
             s["ctx_lists"].close()
 
 
-def test_memory_sharded_forward_at_2_22_two_ranks(gpu_ctx):
-    """The benchmark's bunch and parameters (n = 4, N0 = 125, eta = 0.5, mixed) at N = 2^22 over
-    two ranks, the case with the largest per-rank traversal, on the third call."""
+@pytest.mark.parametrize("N", [2**22, 2**24], ids=["2^22", "2^24"])
+def test_memory_sharded_forward_two_ranks_at_benchmark_sizes(gpu_ctx, N):
+    """The benchmark's bunch and parameters (n = 4, N0 = 125, eta = 0.5, mixed) over two ranks,
+    the case with the largest per-rank traversal, on the third call, with torch's work on its
+    default stream (the contexts must run after it: handle 0 is passed as cudaStreamLegacy)."""
     import fmmb200
     from fmmb200 import beams, sharded
 
-    N = 2**22
     pos, mom = beams.gaussian_bunch(N, seed=0)
     alg = fmmb200.FMMB200(n=4, N0=125, eta=0.5, precision="mixed")
     slots = _slots(pos, mom, [N // 2, N - N // 2])
