@@ -1414,8 +1414,8 @@ __global__ void adj_p2p_rec_kernel(int N, const float4 *__restrict__ prec32x2, c
 // kernel's finite derivative (f = eps^-3/2 times c; the f5 term is formed as
 // f (s^2 (R.c)) and vanishes without overflowing).  The FP32 partial sums of
 // kPbFold tiles at a time are added into FP64 sums in shared memory.  Tiles whose
-// boxes are apart by more than 1/16 of the larger extent form R from the hi parts
-// alone, as in the forward.
+// boxes are apart by more than 1/kHiOnlyGap of the larger extent form R from the hi
+// parts alone, as in the forward.
 constexpr int kPbFold = 8;
 
 template <int G>
@@ -1461,12 +1461,7 @@ __global__ void __launch_bounds__(128)
     s_centre[bb][0] = 0.5 * (sb[0] + sb[3]);
     s_centre[bb][1] = 0.5 * (sb[1] + sb[4]);
     s_centre[bb][2] = 0.5 * (sb[2] + sb[5]);
-    double gap = 0.0, ext = 0.0;
-    for (int d = 0; d < 3; ++d) {
-      gap = fmax(gap, fmax(sb[d] - tbox[3 + d], tbox[d] - sb[3 + d]));
-      ext = fmax(ext, fmax(sb[3 + d] - sb[d], tbox[3 + d] - tbox[d]));
-    }
-    s_near[bb] = !(16.0 * gap > ext);
+    s_near[bb] = p2p_tile_needs_lo(sb, tbox);
     const uint32_t bytes = (uint32_t)(cnt * REC * sizeof(float4));
     mbar_arrive_expect_tx(&bar[bb], bytes);
     bulk_g2s(&buf[bb][0], recb + (int64_t)(slo + woff) * REC, bytes, &bar[bb]);

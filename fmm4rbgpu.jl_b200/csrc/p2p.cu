@@ -235,14 +235,8 @@ __global__ void __launch_bounds__(128) p2p_x2_kernel(const int *__restrict__ lea
     s_centre[bb][0] = 0.5 * (sb[0] + sb[3]);
     s_centre[bb][1] = 0.5 * (sb[1] + sb[4]);
     s_centre[bb][2] = 0.5 * (sb[2] + sb[5]);
-    // Boxes whose gap exceeds 1/16 of the larger extent: every pair difference is at least
-    // that gap, so the hi parts alone give R to ~17 FP32 ulps and the lo parts are skipped.
-    double gap = 0.0, ext = 0.0;
-    for (int d = 0; d < 3; ++d) {
-      gap = fmax(gap, fmax(sb[d] - tbox[3 + d], tbox[d] - sb[3 + d]));
-      ext = fmax(ext, fmax(sb[3 + d] - sb[d], tbox[3 + d] - tbox[d]));
-    }
-    s_near[bb] = !(16.0 * gap > ext);
+    // boxes apart by more than 1/kHiOnlyGap of the larger extent: R from the hi parts alone
+    s_near[bb] = p2p_tile_needs_lo(sb, tbox);
     const uint32_t bytes = (uint32_t)(cnt * REC * sizeof(float4));
     mbar_arrive_expect_tx(&bar[bb], bytes);
     bulk_g2s(&buf[bb][0], rec_x2 + (int64_t)first * REC, bytes, &bar[bb]);

@@ -28,6 +28,27 @@ __device__ __forceinline__ float rsqrt_approx_f32(float x) {
 }
 __device__ __forceinline__ float2 rsqrt2(float2 d) { return make_float2(rsqrt_approx_f32(d.x), rsqrt_approx_f32(d.y)); }
 
+// Mixed P2P and P2P^T tiles whose source and target boxes are apart by more than
+// 1/kHiOnlyGap of the larger extent form every pair difference R from the hi parts of the
+// coordinates alone (the lo parts are skipped).  Every pair of such a tile is at least the gap
+// apart while the coordinates (in the source leaf's frame) are at most about 1.5 extents, so R
+// keeps a relative error below about 3 kHiOnlyGap FP32 ulps (1e-4 at 256), reached only by
+// pairs at the gap itself.  At 256, 87 % of the P2P tiles of the N = 2^24 Gaussian bunch
+// (n = 4, N0 = 125) take the hi path (55 % at 16): the P2P stage drops from 57.0 to 51.7 ms,
+// and the mixed-vs-FP64 error over all particles moves from 2.233e-7 to 2.238e-7 (2^22: Gaussian
+// 1.91e-7 -> 2.04e-7, uniform 2.44e-7 -> 2.45e-7, beamlets 1.84e-7 -> 2.02e-7).
+constexpr double kHiOnlyGap = 256.0;
+
+__device__ __forceinline__ bool p2p_tile_needs_lo(const double *sb, const double *tb) {
+  double gap = 0.0, ext = 0.0;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    gap = fmax(gap, fmax(sb[d] - tb[3 + d], tb[d] - sb[3 + d]));
+    ext = fmax(ext, fmax(sb[3 + d] - sb[d], tb[3 + d] - tb[d]));
+  }
+  return !(kHiOnlyGap * gap > ext);
+}
+
 // The FP32 M2L kernels factor their sums over the source nodes y_b around the target
 // centre (E = x' G - Q and the like), which loses a factor (|x'| + |y|) / |x' - y| of
 // precision for a target node x' and a source node y.  True when that factor stays
