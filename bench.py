@@ -547,18 +547,28 @@ def run_ours(args, world, rank, local):
                      "frac": ach64 / p64.value if p64.value else None, "ms_per_launch": st64["ms_m2l"]}}
     # The FP32 pipe executes one FMA-class operation per lane per cycle, packed or not, so an
     # operation count per evaluation turns the kernel time into the pipe's occupancy:
-    # M2L 15 per evaluation (3 denominator, 2 s^3, 10 factored sums), P2P 31 for tiles near
+    # M2L 15 per evaluation (3 denominator, 2 s^3, 10 factored sums), P2P 30 for tiles near
     # the target leaf (9 for R from hi/lo parts, 3 R.R, 3 u.R, 1 d, 2 s^3, 3 K, 3 E, 6 B) and
-    # 25 for the far ones (R from the hi parts alone); the peak is the measured FMA rate / 2.
+    # 24 for the far ones (R from the hi parts alone); the peak is the measured FMA rate / 2.
     pipe = p32.value * 1e12 / 2.0
     if st["ms_m2l"] > 0 and pipe > 0:
         roof["fp32_pipe_occupancy"] = 15.0 * st["m2l_kernel_evals"] / (st["ms_m2l"] * 1e-3) / pipe
     if st["ms_p2p"] > 0:
         ach_p = 41.0 * st["p2p_kernel_evals"] / (st["ms_p2p"] * 1e-3) / 1e12
+        # the attainable rate of the kernel's own evaluation body (sources in shared memory,
+        # no staging or barriers), for far and near tiles: the ceiling of this instruction mix
+        bfar = ctypes.c_double()
+        bnear = ctypes.c_double()
+        ctx._check(L.fmmb200_measure_p2p_body(ctx.handle, ctypes.byref(bfar), ctypes.byref(bnear)))
+        rate = st["p2p_kernel_evals"] / (st["ms_p2p"] * 1e-3)
         roof["p2p"] = {"kernel": "p2p_x2_kernel (mixed)", "achieved": ach_p, "peak": p32.value, "unit": "TFLOP/s",
                        "frac": ach_p / p32.value if p32.value else None, "ms_per_launch": st["ms_p2p"],
-                       "fp32_pipe_occupancy_if_all_near": 31.0 * st["p2p_kernel_evals"] / (st["ms_p2p"] * 1e-3)
-                       / pipe if pipe > 0 else None}
+                       "fp32_pipe_occupancy_if_all_near": 30.0 * rate / pipe if pipe > 0 else None,
+                       "fp32_pipe_occupancy_if_all_far": 24.0 * rate / pipe if pipe > 0 else None,
+                       "evals_per_s": rate, "body_rate_far": bfar.value, "body_rate_near": bnear.value,
+                       "frac_of_body_rate_far": rate / bfar.value if bfar.value else None,
+                       "frac_of_body_rate_near": rate / bnear.value if bnear.value else None,
+                       "min_ms_at_body_rate_far": st["p2p_kernel_evals"] / bfar.value * 1e3 if bfar.value else None}
 
     # end to end through the host-pointer C-ABI (pinned host buffers)
     e2e = None

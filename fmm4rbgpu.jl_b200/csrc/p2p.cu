@@ -196,6 +196,59 @@ __global__ void __launch_bounds__(128) p2p_kernel(const int *__restrict__ leaf_i
   }
 }
 
+// The evaluation body of the mixed kernels, shared with the probe of its attainable rate.
+// A pair of targets (the two lanes of FP32x2) in a source leaf's frame, as hi + lo parts.
+struct P2PTargets {
+  float2 xh, yh, zh, xl, yl, zl;
+};
+// FP32 partial sums of a target pair: E, and B = bp - bm.
+struct P2PAcc {
+  float2 e0, e1, e2, bp0, bp1, bp2, bm0, bm1, bm2;
+};
+// One staged source record: -hi, -lo coordinates (lo only for NEAR), gamma, u.
+struct P2PSource {
+  float2 xh, yh, zh, xl, yl, zl, gam, ux, uy, uz;
+};
+
+template <bool NEAR>
+__device__ __forceinline__ P2PSource p2p_x2_load(const float4 *__restrict__ r) {
+  const float4 r0 = r[0], r1 = r[1], r3 = r[3], r4 = r[4];
+  const float4 r2 = NEAR ? r[2] : make_float4(0.f, 0.f, 0.f, 0.f);
+  return P2PSource{lo2(r0), hi2(r0), lo2(r1), hi2(r1), lo2(r2), hi2(r2), lo2(r3), hi2(r3), lo2(r4), hi2(r4)};
+}
+
+// E += gamma K, B += u x K with K = s^3 R, s = (R.R + (u.R)^2 + eps)^(-1/2), for one source and
+// one target pair.  R = (target hi - source hi) + (target lo - source lo) when NEAR, else from
+// the hi parts alone; the record holds -hi, -lo.
+template <bool NEAR>
+__device__ __forceinline__ void p2p_x2_eval(const P2PSource &q, const P2PTargets &t, float2 eps, P2PAcc &a) {
+  float2 rx, ry, rz;
+  if constexpr (NEAR) {
+    rx = add2(add2(t.xh, q.xh), add2(t.xl, q.xl));
+    ry = add2(add2(t.yh, q.yh), add2(t.yl, q.yl));
+    rz = add2(add2(t.zh, q.zh), add2(t.zl, q.zl));
+  } else {
+    rx = add2(t.xh, q.xh);
+    ry = add2(t.yh, q.yh);
+    rz = add2(t.zh, q.zh);
+  }
+  const float2 rre = fma2(rx, rx, fma2(ry, ry, fma2(rz, rz, eps)));
+  const float2 pr = fma2(q.uz, rz, fma2(q.uy, ry, mul2(q.ux, rx)));
+  const float2 d = fma2(pr, pr, rre);
+  const float2 sv = rsqrt2(d);
+  const float2 s3 = mul2(mul2(sv, sv), sv);
+  const float2 kx = mul2(s3, rx), ky = mul2(s3, ry), kz = mul2(s3, rz);  // K = s^3 R
+  a.e0 = fma2(q.gam, kx, a.e0);
+  a.e1 = fma2(q.gam, ky, a.e1);
+  a.e2 = fma2(q.gam, kz, a.e2);
+  a.bp0 = fma2(q.uy, kz, a.bp0);  // B = u x K as (bp - bm)
+  a.bm0 = fma2(q.uz, ky, a.bm0);
+  a.bp1 = fma2(q.uz, kx, a.bp1);
+  a.bm1 = fma2(q.ux, kz, a.bm1);
+  a.bp2 = fma2(q.ux, ky, a.bp2);
+  a.bm2 = fma2(q.uy, kx, a.bm2);
+}
+
 template <int G, int TP>
 __global__ void __launch_bounds__(128) p2p_x2_kernel(const int *__restrict__ leaf_ids, int leaf0,
                                                      const int *__restrict__ lohi, const int *__restrict__ ptr,
@@ -269,9 +322,9 @@ __global__ void __launch_bounds__(128) p2p_x2_kernel(const int *__restrict__ lea
     }
     // FP32 partial sums over kP2PFold tiles, then added into the FP64 sums
     const float2 z = make_float2(0.f, 0.f);
-    float2 e0[TP], e1[TP], e2[TP], bp0[TP], bp1[TP], bp2[TP], bm0[TP], bm1[TP], bm2[TP];
+    P2PAcc acc[TP];
 #pragma unroll
-    for (int t = 0; t < TP; ++t) e0[t] = e1[t] = e2[t] = bp0[t] = bp1[t] = bp2[t] = bm0[t] = bm1[t] = bm2[t] = z;
+    for (int t = 0; t < TP; ++t) acc[t] = P2PAcc{z, z, z, z, z, z, z, z, z};
     for (int i = 0; i < W; ++i, ++it) {
       const int bb = it & 1;
       if (tid == 0 && i + 1 < W) {
@@ -283,17 +336,18 @@ __global__ void __launch_bounds__(128) p2p_x2_kernel(const int *__restrict__ lea
         const int cnt = s_cnt[bb];
         // the targets in the source leaf's frame, as hi + lo
         const double scx = s_centre[bb][0], scy = s_centre[bb][1], scz = s_centre[bb][2];
-        float2 xh[TP], yh[TP], zh[TP], xl[TP], yl[TP], zl[TP];
+        P2PTargets tg[TP];
 #pragma unroll
         for (int t = 0; t < TP; ++t) {
           const double dx0 = tX[2 * t] - scx, dy0 = tY[2 * t] - scy, dz0 = tZ[2 * t] - scz;
           const double dx1 = tX[2 * t + 1] - scx, dy1 = tY[2 * t + 1] - scy, dz1 = tZ[2 * t + 1] - scz;
-          xh[t] = make_float2((float)dx0, (float)dx1);
-          yh[t] = make_float2((float)dy0, (float)dy1);
-          zh[t] = make_float2((float)dz0, (float)dz1);
-          xl[t] = make_float2((float)(dx0 - (double)xh[t].x), (float)(dx1 - (double)xh[t].y));
-          yl[t] = make_float2((float)(dy0 - (double)yh[t].x), (float)(dy1 - (double)yh[t].y));
-          zl[t] = make_float2((float)(dz0 - (double)zh[t].x), (float)(dz1 - (double)zh[t].y));
+          P2PTargets &o = tg[t];
+          o.xh = make_float2((float)dx0, (float)dx1);
+          o.yh = make_float2((float)dy0, (float)dy1);
+          o.zh = make_float2((float)dz0, (float)dz1);
+          o.xl = make_float2((float)(dx0 - (double)o.xh.x), (float)(dx1 - (double)o.xh.y));
+          o.yl = make_float2((float)(dy0 - (double)o.yh.x), (float)(dy1 - (double)o.yh.y));
+          o.zl = make_float2((float)(dz0 - (double)o.zh.x), (float)(dz1 - (double)o.zh.y));
         }
         const float2 eps = dup2((float)kEps64);
         const float4 *S = &buf[bb][0];
@@ -301,39 +355,9 @@ __global__ void __launch_bounds__(128) p2p_x2_kernel(const int *__restrict__ lea
           constexpr bool NEAR = decltype(NEARC)::value;
 #pragma unroll 2
           for (int j = g; j < cnt; j += G) {
-            const float4 *r = S + j * REC;
-            const float4 r0 = r[0], r1 = r[1], r3 = r[3], r4 = r[4];
-            const float4 r2 = NEAR ? r[2] : make_float4(0.f, 0.f, 0.f, 0.f);
-            const float2 gam = lo2(r3), ux = hi2(r3), uy = lo2(r4), uz = hi2(r4);
+            const P2PSource q = p2p_x2_load<NEAR>(S + j * REC);
 #pragma unroll
-            for (int t = 0; t < TP; ++t) {
-              // R = (target hi - source hi) + (target lo - source lo); the record holds -hi, -lo
-              float2 rx, ry, rz;
-              if constexpr (NEAR) {
-                rx = add2(add2(xh[t], lo2(r0)), add2(xl[t], hi2(r1)));
-                ry = add2(add2(yh[t], hi2(r0)), add2(yl[t], lo2(r2)));
-                rz = add2(add2(zh[t], lo2(r1)), add2(zl[t], hi2(r2)));
-              } else {
-                rx = add2(xh[t], lo2(r0));
-                ry = add2(yh[t], hi2(r0));
-                rz = add2(zh[t], lo2(r1));
-              }
-              const float2 rre = fma2(rx, rx, fma2(ry, ry, fma2(rz, rz, eps)));
-              const float2 pr = fma2(uz, rz, fma2(uy, ry, mul2(ux, rx)));
-              const float2 d = fma2(pr, pr, rre);
-              const float2 s = rsqrt2(d);
-              const float2 s3 = mul2(mul2(s, s), s);
-              const float2 kx = mul2(s3, rx), ky = mul2(s3, ry), kz = mul2(s3, rz);  // K = s^3 R
-              e0[t] = fma2(gam, kx, e0[t]);
-              e1[t] = fma2(gam, ky, e1[t]);
-              e2[t] = fma2(gam, kz, e2[t]);
-              bp0[t] = fma2(uy, kz, bp0[t]);  // B = u x K as (bp - bm)
-              bm0[t] = fma2(uz, ky, bm0[t]);
-              bp1[t] = fma2(uz, kx, bp1[t]);
-              bm1[t] = fma2(ux, kz, bm1[t]);
-              bp2[t] = fma2(ux, ky, bp2[t]);
-              bm2[t] = fma2(uy, kx, bm2[t]);
-            }
+            for (int t = 0; t < TP; ++t) p2p_x2_eval<NEAR>(q, tg[t], eps, acc[t]);
           }
         };
         if (s_near[bb])
@@ -344,14 +368,14 @@ __global__ void __launch_bounds__(128) p2p_x2_kernel(const int *__restrict__ lea
       if ((i + 1) % kP2PFold == 0 || i + 1 == W) {
 #pragma unroll
         for (int t = 0; t < TP; ++t) {
-          const float2 part[6] = {e0[t], e1[t], e2[t], sub2(bp0[t], bm0[t]), sub2(bp1[t], bm1[t]),
-                                  sub2(bp2[t], bm2[t])};
+          const P2PAcc &a = acc[t];
+          const float2 part[6] = {a.e0, a.e1, a.e2, sub2(a.bp0, a.bm0), sub2(a.bp1, a.bm1), sub2(a.bp2, a.bm2)};
 #pragma unroll
           for (int q = 0; q < 6; ++q) {
             s_acc[12 * t + q][tid] += (double)part[q].x;
             s_acc[12 * t + 6 + q][tid] += (double)part[q].y;
           }
-          e0[t] = e1[t] = e2[t] = bp0[t] = bp1[t] = bp2[t] = bm0[t] = bm1[t] = bm2[t] = z;
+          acc[t] = P2PAcc{z, z, z, z, z, z, z, z, z};
         }
       }
       __syncthreads();  // buffer bb is refilled two iterations later
@@ -387,6 +411,39 @@ __global__ void __launch_bounds__(128) p2p_x2_kernel(const int *__restrict__ lea
       }
     }
   }
+}
+
+// The attainable rate of the mixed evaluation body on this GPU: the kernel's own load and
+// evaluation code (p2p_x2_load / p2p_x2_eval) over 64 synthetic source records held in
+// shared memory, G = 4 lanes per target pair as for leaves of 64, looped without staging,
+// barriers or folds.  out: one value per thread, so that nothing is dead code.
+template <bool NEAR>
+__global__ void __launch_bounds__(128) p2p_body_probe_kernel(int reps, float *__restrict__ out) {
+  constexpr int NS = 64, G = 4;
+  __shared__ __align__(16) float4 S[NS * 5];
+  for (int j = threadIdx.x; j < NS; j += blockDim.x) {
+    const float x = 0.3f * __cosf((float)j), y = 0.3f * __sinf((float)j), zz = 0.01f * (float)j / NS;
+    const float xl = 1e-9f * (float)(j % 3), yl = -1e-9f * (float)(j % 5), zl = 2e-9f;
+    S[5 * j + 0] = make_float4(-x, -x, -y, -y);
+    S[5 * j + 1] = make_float4(-zz, -zz, -xl, -xl);
+    S[5 * j + 2] = make_float4(-yl, -yl, -zl, -zl);
+    S[5 * j + 3] = make_float4(200.f, 200.f, 0.01f, 0.01f);
+    S[5 * j + 4] = make_float4(-0.02f, -0.02f, 199.9f, 199.9f);
+  }
+  __syncthreads();
+  const int g = threadIdx.x % G, w = threadIdx.x / G;
+  const P2PTargets t{make_float2(0.5f + 0.001f * w, 0.52f + 0.001f * w), make_float2(-0.2f, -0.21f),
+                     make_float2(0.05f, 0.04f), make_float2(1e-9f, -1e-9f), make_float2(0.f, 1e-9f),
+                     make_float2(-2e-9f, 0.f)};
+  const float2 z = make_float2(0.f, 0.f), eps = dup2((float)kEps64);
+  P2PAcc a{z, z, z, z, z, z, z, z, z};
+  for (int r = 0; r < reps; ++r) {
+#pragma unroll 2
+    for (int j = g; j < NS; j += G) p2p_x2_eval<NEAR>(p2p_x2_load<NEAR>(S + 5 * j), t, eps, a);
+  }
+  const float2 v = add2(add2(add2(a.e0, a.e1), add2(a.e2, a.bp0)),
+                        add2(add2(a.bp1, a.bp2), add2(add2(a.bm0, a.bm1), a.bm2)));
+  out[(int64_t)blockIdx.x * blockDim.x + threadIdx.x] = v.x + v.y;
 }
 
 template <int G>
@@ -434,3 +491,46 @@ int launch_p2p(Ctx *ctx, bool mixed, const int *d_leaf_ids, int64_t nleaf, bool 
 }
 
 }  // namespace fmmb200
+
+using namespace fmmb200;
+
+extern "C" {
+
+int fmmb200_measure_p2p_body(fmmb200_ctx *ctx, double *far_evals_per_s, double *near_evals_per_s) {
+  if (!ctx) return FMMB200_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(ctx->device);
+  int nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->device);
+  // six CTAs of 128 threads per SM: the residency of p2p_x2_kernel<4, 1> (80 registers)
+  const int threads = 128, blocks = nsm * 6, reps = 256;
+  float *out;
+  FMM_TRY(ctx->ensure("p2p_probe_out", (int64_t)threads * blocks, &out));
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  // evaluations per launch: every thread holds a target pair and sees 64 / 4 sources per rep
+  const double evals = 2.0 * (64 / 4) * (double)reps * threads * blocks;
+  double best[2] = {0.0, 0.0};
+  for (int rep = 0; rep < 4; ++rep) {
+    for (int k = 0; k < 2; ++k) {
+      cudaEventRecord(a, ctx->stream);
+      if (k == 0)
+        p2p_body_probe_kernel<false><<<blocks, threads, 0, ctx->stream>>>(reps, out);
+      else
+        p2p_body_probe_kernel<true><<<blocks, threads, 0, ctx->stream>>>(reps, out);
+      cudaEventRecord(b, ctx->stream);
+      cudaEventSynchronize(b);
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, a, b);
+      if (rep > 0 && ms > 0.f && evals / (ms * 1e-3) > best[k]) best[k] = evals / (ms * 1e-3);
+    }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  FMM_TRY(ctx->check_launch("p2p_body_probe_kernel", 8));
+  if (far_evals_per_s) *far_evals_per_s = best[0];
+  if (near_evals_per_s) *near_evals_per_s = best[1];
+  return FMMB200_OK;
+}
+
+}  // extern "C"

@@ -105,6 +105,7 @@ SIGNATURES = {
     "fmmb200_direct": (ctypes.c_int, [c_vp, c_i64, p_f64, p_f64, c_f64, c_f64, c_i64, p_i64, p_f64, p_f64]),
     "fmmb200_direct_device": (ctypes.c_int, [c_vp, c_i64, c_vp, c_vp, c_f64, c_f64, c_i64, c_vp, c_vp, c_vp]),
     "fmmb200_measure_fma_peak": (ctypes.c_int, [c_vp, p_f64, p_f64, p_f64]),
+    "fmmb200_measure_p2p_body": (ctypes.c_int, [c_vp, p_f64, p_f64]),
     "fmmb200_set_m2l_engine": (ctypes.c_int, [c_vp, ctypes.c_int]),
     "fmmb200_set_tree_reuse": (ctypes.c_int, [c_vp, ctypes.c_int]),
     "fmmb200_set_shard": (ctypes.c_int, [c_vp, ctypes.c_int, ctypes.c_int]),

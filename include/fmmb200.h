@@ -302,6 +302,13 @@ int fmmb200_shard_evaluate(fmmb200_ctx *ctx, int32_t L, int32_t rank, int64_t ma
                            const int32_t *d_p2p_ptr, const int32_t *d_p2p_src, int64_t np2p,
                            double charge, double lambda, double *d_efields, double *d_bfields);
 
+/* Attainable rate (kernel evaluations per second) of the mixed P2P kernel's evaluation body
+ * on this device: the kernel's own per-source load and evaluation code over source records
+ * held in shared memory, at the kernel's residency (six CTAs of 128 threads per SM), with no
+ * staging, barriers or FP64 folds.  far: R from the hi parts (tiles apart by more than
+ * 1/256 of their extent); near: from hi and lo parts.  The ceiling of p2p_x2_kernel's
+ * rate for this instruction mix; no counterpart in the reference. */
+int fmmb200_measure_p2p_body(fmmb200_ctx *ctx, double *far_evals_per_s, double *near_evals_per_s);
 /* Measured CUDA-core FMA throughput (TFLOP/s, 2 flops per FMA) of the device with
  * scalar FP64, scalar FP32 and packed FP32x2 (FFMA2) chains: the roofline
  * denominators of the M2L / P2P kernels. */

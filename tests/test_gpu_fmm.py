@@ -350,3 +350,33 @@ def test_tree_reuse_is_exact(gpu_ctx):
     finally:
         gpu_ctx.set_tree_reuse(False)
         fresh.close()
+
+
+def test_roofline_probes_bound_the_kernels(gpu_ctx):
+    """The measured ceilings the benchmark divides by: the FMA peaks (scalar FP64, scalar FP32,
+    packed FP32x2) and the attainable rate of the mixed P2P evaluation body, which must bound
+    the P2P kernel's own rate on a beam whose P2P stage is a few ms."""
+    import ctypes
+
+    import fmmb200
+
+    L = gpu_ctx._lib
+    p64, p32, p2 = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+    gpu_ctx._check(L.fmmb200_measure_fma_peak(gpu_ctx.handle, ctypes.byref(p64), ctypes.byref(p32), ctypes.byref(p2)))
+    assert 0 < p64.value < p32.value and p2.value > 0
+    far, near = ctypes.c_double(), ctypes.c_double()
+    gpu_ctx._check(L.fmmb200_measure_p2p_body(gpu_ctx.handle, ctypes.byref(far), ctypes.byref(near)))
+    assert 0 < near.value < far.value
+    # a body of 24 (far) FP32 operations per evaluation cannot beat the FP32 pipe
+    assert 24.0 * far.value < 1.05 * p32.value * 1e12 / 2.0
+    from fmmb200 import beams
+
+    pos, mom = beams.gaussian_bunch(2**20, seed=3)
+    gpu_ctx.set_timing(True)
+    try:
+        gpu_ctx.forward(pos, mom, fmmb200.FMMB200(n=4, N0=125, eta=0.5, precision="mixed"))
+        st = gpu_ctx.stats()
+    finally:
+        gpu_ctx.set_timing(False)
+    rate = st["p2p_kernel_evals"] / (st["ms_p2p"] * 1e-3)
+    assert 0 < rate < far.value
