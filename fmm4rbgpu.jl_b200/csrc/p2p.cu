@@ -16,7 +16,10 @@
 // FP64 form (p2p_kernel): 64-byte records, double arithmetic.
 // Mixed form (p2p_x2_kernel): each pair of targets of a lane group is evaluated in
 // the two lanes of packed FP32x2 instructions on coordinates relative to the
-// source leaf's box centre, each stored as a hi + lo pair of floats.  Per tile
+// source leaf's box centre, each stored as a hi + lo pair of floats.  Its G lanes of a
+// target group are TG = 128 / G threads apart, so a warp's threads share one source lane
+// and every record load is a broadcast; the lanes' FP64 sums are combined through shared
+// memory in the pairwise order of an xor butterfly over adjacent lanes.  Per tile
 // the targets are moved into the source's frame in FP64 once and split the same
 // way; every pair difference R = (X_hi - x_hi) + (X_lo - x_lo) is then formed to
 // ~1 ulp of |R| even for very close pairs (the hi difference is exact,
@@ -196,6 +199,15 @@ __global__ void __launch_bounds__(128) p2p_kernel(const int *__restrict__ leaf_i
   }
 }
 
+// Sum of G values v[0], v[stride], ..., pairwise in index order: ((v0 + v1) + (v2 + v3)) + ...
+template <int G>
+__device__ __forceinline__ double lane_tree_sum(const double *v, int stride) {
+  if constexpr (G == 1)
+    return v[0];
+  else
+    return lane_tree_sum<G / 2>(v, stride) + lane_tree_sum<G / 2>(v + (G / 2) * stride, stride);
+}
+
 // The evaluation body of the mixed kernels, shared with the probe of its attainable rate.
 // A pair of targets (the two lanes of FP32x2) in a source leaf's frame, as hi + lo parts.
 struct P2PTargets {
@@ -265,7 +277,9 @@ __global__ void __launch_bounds__(128) p2p_x2_kernel(const int *__restrict__ lea
   __shared__ double s_acc[12 * TP][128];  // per thread: E, B of its 2 TP targets, FP64 sums over tiles
 
   const int tid = threadIdx.x, BT = blockDim.x, TG = BT / G;
-  const int tl = tid / G, g = tid % G;
+  // source lane g = tid / TG: the TG threads of a lane, whole warps when TG >= 32, read
+  // the same staged source record at once (one shared-memory broadcast per load)
+  const int tl = tid % TG, g = tid / TG;
   const int c = leaf_ids ? leaf_ids[blockIdx.x] : leaf0 + blockIdx.x;
   const double *tbox = bbox + 6 * (int64_t)c;
   const int tlo = lohi[2 * c], thi = lohi[2 * c + 1], tcnt = thi - tlo + 1;
@@ -380,21 +394,18 @@ __global__ void __launch_bounds__(128) p2p_x2_kernel(const int *__restrict__ lea
       }
       __syncthreads();  // buffer bb is refilled two iterations later
     }
-    // combine the G lanes of each target group (warp shuffles), FP64 result
+    // combine the G lanes of each target group, FP64 result: pairwise in lane order, the
+    // order of an xor butterfly over adjacent lanes
+    __syncthreads();  // every lane's sums are in s_acc
 #pragma unroll
     for (int t = 0; t < TP; ++t) {
       double v0[6], v1[6];
-#pragma unroll
-      for (int q = 0; q < 6; ++q) {
-        v0[q] = s_acc[12 * t + q][tid];
-        v1[q] = s_acc[12 * t + 6 + q][tid];
-#pragma unroll
-        for (int o = 1; o < G; o <<= 1) {
-          v0[q] += __shfl_xor_sync(0xffffffffu, v0[q], o);
-          v1[q] += __shfl_xor_sync(0xffffffffu, v1[q], o);
-        }
-      }
       if (g == 0) {
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+          v0[q] = lane_tree_sum<G>(&s_acc[12 * t + q][tl], TG);
+          v1[q] = lane_tree_sum<G>(&s_acc[12 * t + 6 + q][tl], TG);
+        }
 #pragma unroll
         for (int q = 0; q < 6; ++q) {
           if (act[2 * t]) {
@@ -410,12 +421,13 @@ __global__ void __launch_bounds__(128) p2p_x2_kernel(const int *__restrict__ lea
         }
       }
     }
+    __syncthreads();  // s_acc is reset by the next round
   }
 }
 
 // The attainable rate of the mixed evaluation body on this GPU: the kernel's own load and
 // evaluation code (p2p_x2_load / p2p_x2_eval) over 64 synthetic source records held in
-// shared memory, G = 4 lanes per target pair as for leaves of 64, looped without staging,
+// shared memory, G = 4 source lanes (one per warp) as for leaves of 64, looped without staging,
 // barriers or folds.  out: one value per thread, so that nothing is dead code.
 template <bool NEAR>
 __global__ void __launch_bounds__(128) p2p_body_probe_kernel(int reps, float *__restrict__ out) {
@@ -431,7 +443,7 @@ __global__ void __launch_bounds__(128) p2p_body_probe_kernel(int reps, float *__
     S[5 * j + 4] = make_float4(-0.02f, -0.02f, 199.9f, 199.9f);
   }
   __syncthreads();
-  const int g = threadIdx.x % G, w = threadIdx.x / G;
+  const int g = threadIdx.x / (blockDim.x / G), w = threadIdx.x % (blockDim.x / G);  // the kernel's lanes
   const P2PTargets t{make_float2(0.5f + 0.001f * w, 0.52f + 0.001f * w), make_float2(-0.2f, -0.21f),
                      make_float2(0.05f, 0.04f), make_float2(1e-9f, -1e-9f), make_float2(0.f, 1e-9f),
                      make_float2(-2e-9f, 0.f)};
