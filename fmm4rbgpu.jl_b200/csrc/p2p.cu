@@ -7,19 +7,17 @@
 // Design: one CTA per target leaf.  Particles are stored in tree order, so every
 // source leaf is one contiguous range of records: tiles of up to 128 source
 // records are bulk-copied (TMA) into a double buffer guarded by mbarriers.  G
-// adjacent lanes share two target particles (both use every staged source
-// record) and split the sources; their partial fields are combined with warp
-// shuffles.  G is chosen from the leaf size so that small leaves (64 particles
-// at N0 = 125) still fill the CTA -- the reference launches N0 threads per
-// leaf and leaves about half of them idle.
+// source lanes share the targets (both use every staged source record) and split
+// the sources.  A lane is TG = 128 / G threads, whole warps for G <= 4, so every
+// record load is a shared-memory broadcast; the lanes' FP64 sums are combined
+// through shared memory, pairwise in lane order.  G is chosen from the leaf size
+// so that small leaves (64 particles at N0 = 125) still fill the CTA -- the
+// reference launches N0 threads per leaf and leaves about half of them idle.
 //
 // FP64 form (p2p_kernel): 64-byte records, double arithmetic.
 // Mixed form (p2p_x2_kernel): each pair of targets of a lane group is evaluated in
 // the two lanes of packed FP32x2 instructions on coordinates relative to the
-// source leaf's box centre, each stored as a hi + lo pair of floats.  Its G lanes of a
-// target group are TG = 128 / G threads apart, so a warp's threads share one source lane
-// and every record load is a broadcast; the lanes' FP64 sums are combined through shared
-// memory in the pairwise order of an xor butterfly over adjacent lanes.  Per tile
+// source leaf's box centre, each stored as a hi + lo pair of floats.  Per tile
 // the targets are moved into the source's frame in FP64 once and split the same
 // way; every pair difference R = (X_hi - x_hi) + (X_lo - x_lo) is then formed to
 // ~1 ulp of |R| even for very close pairs (the hi difference is exact,
@@ -78,6 +76,15 @@ struct TileCursor {
   }
 };
 
+// Sum of G values v[0], v[stride], ..., pairwise in index order: ((v0 + v1) + (v2 + v3)) + ...
+template <int G>
+__device__ __forceinline__ double lane_tree_sum(const double *v, int stride) {
+  if constexpr (G == 1)
+    return v[0];
+  else
+    return lane_tree_sum<G / 2>(v, stride) + lane_tree_sum<G / 2>(v + (G / 2) * stride, stride);
+}
+
 template <int G>
 __global__ void __launch_bounds__(128) p2p_kernel(const int *__restrict__ leaf_ids, int leaf0,
                                                   const int *__restrict__ lohi, const int *__restrict__ ptr,
@@ -89,9 +96,12 @@ __global__ void __launch_bounds__(128) p2p_kernel(const int *__restrict__ leaf_i
   __shared__ __align__(8) uint64_t bar[2];
   __shared__ int s_cnt[2];
   __shared__ int s_warp[33];
+  __shared__ double s_red[kTT * 6][128];  // per thread: E, B of its targets, for the lane sum
 
   const int tid = threadIdx.x, BT = blockDim.x, TG = BT / G;
-  const int tl = tid / G, g = tid % G;
+  // source lane g = tid / TG: a warp's threads share one lane (TG >= 32), so every staged
+  // record load is a broadcast
+  const int tl = tid % TG, g = tid / TG;
   const int c = leaf_ids ? leaf_ids[blockIdx.x] : leaf0 + blockIdx.x;
   const int tlo = lohi[2 * c], thi = lohi[2 * c + 1], tcnt = thi - tlo + 1;
   const int p0 = ptr[c], np = ptr[c + 1] - p0;
@@ -176,36 +186,27 @@ __global__ void __launch_bounds__(128) p2p_kernel(const int *__restrict__ leaf_i
       }
       __syncthreads();  // buffer bb is refilled two iterations later
     }
-    // combine the G lanes of each target group (warp shuffles)
+    // combine the G lanes of each target group through shared memory, pairwise in lane
+    // order (the order of an xor butterfly over adjacent lanes)
+#pragma unroll
+    for (int u = 0; u < kTT; ++u)
+#pragma unroll
+      for (int q = 0; q < 6; ++q) s_red[u * 6 + q][tid] = acc[u][q];
+    __syncthreads();
 #pragma unroll
     for (int u = 0; u < kTT; ++u) {
-      double v[6];
-#pragma unroll
-      for (int q = 0; q < 6; ++q) {
-        v[q] = acc[u][q];
-#pragma unroll
-        for (int o = 1; o < G; o <<= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
-      }
       if (active[u] && g == 0) {
         const int64_t pj = tlo + ti[u];
 #pragma unroll
         for (int q = 0; q < 6; ++q) {
-          double o = v[q];
+          double o = lane_tree_sum<G>(&s_red[u * 6 + q][tl], TG);
           if (accumulate) o += near[(int64_t)q * N + pj];
           near[(int64_t)q * N + pj] = o;
         }
       }
     }
+    __syncthreads();  // s_red is rewritten by the next round
   }
-}
-
-// Sum of G values v[0], v[stride], ..., pairwise in index order: ((v0 + v1) + (v2 + v3)) + ...
-template <int G>
-__device__ __forceinline__ double lane_tree_sum(const double *v, int stride) {
-  if constexpr (G == 1)
-    return v[0];
-  else
-    return lane_tree_sum<G / 2>(v, stride) + lane_tree_sum<G / 2>(v + (G / 2) * stride, stride);
 }
 
 // The evaluation body of the mixed kernels, shared with the probe of its attainable rate.
