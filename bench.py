@@ -80,6 +80,7 @@ def parse():
                     help="one more reference-arm evaluation at this size, outside the timed steps, so that "
                          "the growth of the CPU cost per particle with N is visible (0: skip)")
     ap.add_argument("--skip-nsweep", action="store_true")
+    ap.add_argument("--skip-configs", action="store_true", help="skip the other benchmark configurations")
     ap.add_argument("--nsweep", default="2:0.5,3:0.5,4:0.5,5:0.5,6:0.5,4:0.4,4:0.3,4:0.25,4:0.2",
                     help="n:eta settings of the accuracy/throughput sweep (the FMM's error against the direct sum "
                          "has a floor set by eta, from the mean momentum in its far-field kernel, so the sweep "
@@ -383,6 +384,68 @@ def run_large(args, ctx, stream, dev):
     return out
 
 
+def run_configs(args, stream, dev):
+    """The other configurations of the benchmark list: per configuration the mixed and FP64
+    forwards (device-resident, each on a context of its own, with its device bytes), the
+    mixed-vs-FP64 error, and for the two adjoint configurations the mixed forward + adjoint time
+    and the mixed context's device bytes with the adjoint's buffers."""
+    import torch
+
+    import fmmb200
+    from fmmb200 import beams
+
+    def rel(a, b):
+        nb = float(torch.linalg.norm(b))
+        return float(torch.linalg.norm(a - b) / nb) if nb > 0 else float(torch.linalg.norm(a))
+
+    cases = [("uniform_65536", beams.uniform, 65536, 4, 125, False),
+             ("gauss_1048576", beams.gaussian_bunch, 2**20, 4, 125, False),
+             ("adjoint_gauss_262144", beams.gaussian_bunch, 262144, 4, 125, True),
+             ("beamlets_4194304_n5_N0_64", beams.beamlets, 2**22, 5, 64, True)]
+    out = {}
+    for name, gen, N, n, N0, adjoint in cases:
+        pos_h, mom_h = gen(N, seed=args.seed)
+        pos = torch.from_numpy(pos_h).to(dev)
+        mom = torch.from_numpy(mom_h).to(dev)
+        res = {"N": N, "n": n, "N0": N0, "eta": args.eta}
+        fields, ctxs = {}, {}
+        for prec in ("mixed", "fp64"):
+            # a context per precision, so that its device bytes are this run's alone
+            ctxs[prec] = c = fmmb200.Context(dev.index)
+            c.set_stream(stream.cuda_stream)
+            alg = fmmb200.FMMB200(n=n, N0=N0, eta=args.eta, precision=prec)
+            e, b = torch.empty_like(pos), torch.empty_like(pos)
+            ms = _events_ms(stream, lambda: c.forward_device(N, pos.data_ptr(), mom.data_ptr(), e.data_ptr(),
+                                                             b.data_ptr(), alg), 3, 2)
+            res[prec] = {"ms_per_step": ms, "value": N / (ms * 1e-3), "device_bytes": int(c.stats()["device_bytes"])}
+            fields[prec] = (e, b)
+        ctx = ctxs["mixed"]
+        res["mixed_vs_fp64"] = {"E": rel(fields["mixed"][0], fields["fp64"][0]),
+                                "B": rel(fields["mixed"][1], fields["fp64"][1])}
+        if adjoint:
+            alg = fmmb200.FMMB200(n=n, N0=N0, eta=args.eta, precision="mixed")
+            e, b = fields["mixed"]
+            gen_t = torch.Generator(device=dev).manual_seed(args.seed + 1)
+            gE = torch.randn((N, 3), dtype=torch.float64, device=dev, generator=gen_t)
+            gB = torch.randn((N, 3), dtype=torch.float64, device=dev, generator=gen_t)
+            gx, gu = torch.empty_like(gE), torch.empty_like(gE)
+
+            def fb():
+                ctx.forward_device(N, pos.data_ptr(), mom.data_ptr(), e.data_ptr(), b.data_ptr(), alg,
+                                   save_for_backward=True)
+                ctx.backward_device(gE.data_ptr(), gB.data_ptr(), gx.data_ptr(), gu.data_ptr())
+
+            ms = _events_ms(stream, fb, 2, 2)
+            res["fwd_bwd_mixed"] = {"ms_per_step": ms, "ratio_to_forward": ms / res["mixed"]["ms_per_step"],
+                                    "grad_finite": bool(torch.isfinite(gx).all() and torch.isfinite(gu).all())}
+            res["device_bytes_with_backward"] = int(ctx.stats()["device_bytes"])
+        out[name] = res
+        for c in ctxs.values():
+            c.close()
+        del pos, mom, fields
+    return out
+
+
 # ---------------------------------------------------------------------------- our arm
 def run_ours(args, world, rank, local):
     import torch
@@ -603,10 +666,13 @@ def run_ours(args, world, rank, local):
 
     nsweep = None
     large = None
+    configs = None
     if world == 1 and not args.skip_nsweep:
         nsweep = run_nsweep(args, ctx, stream, N, pos, mom, tg, Ed, Bd)
     if world == 1 and args.large_N > 0:
         large = run_large(args, ctx, stream, dev)
+    if world == 1 and not args.skip_configs:
+        configs = run_configs(args, stream, dev)
 
     cpu = None
     if rank == 0 and world == 1 and not args.skip_cpu_baseline:
@@ -637,6 +703,7 @@ def run_ours(args, world, rank, local):
             "reuse": reuse,
             "nsweep": nsweep,
             "large": large,
+            "configs": configs,
             "roofline": roof,
             "cpu_baseline": cpu,
             "e2e": e2e,
