@@ -180,16 +180,22 @@ __global__ void node_kernel(int l, int ml, int N, const double *__restrict__ pos
   }
 }
 
-// flag[p] = 1 if particle p goes to the left child of its level-l node.
+// flag[p] = 1 if particle p goes to the left child of its level-l node.  Each thread takes
+// kFlagItems positions blockDim apart and descends again only past its node's end (a node
+// of a global level holds thousands of particles).
+constexpr int kFlagItems = 4;
 __global__ void flag_kernel(int l, int N, const uint32_t *__restrict__ lists, const int *__restrict__ split,
                             uint8_t *__restrict__ flag) {
-  int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= N) return;
-  int lo, hi;
-  int k = descend(j, l, N, &lo, &hi);
-  int mid = (lo + hi) >> 1;
-  uint32_t p = lists[(int64_t)split[k] * N + j];
-  flag[p] = (j <= mid) ? 1 : 0;
+  const int j0 = blockIdx.x * blockDim.x * kFlagItems + threadIdx.x;
+  int lo = 0, hi = -1, k = 0;
+#pragma unroll
+  for (int i = 0; i < kFlagItems; ++i) {
+    const int j = j0 + i * blockDim.x;
+    if (j >= N) break;
+    if (j > hi) k = descend(j, l, N, &lo, &hi);
+    const uint32_t p = lists[(int64_t)split[k] * N + j];
+    flag[p] = (j <= ((lo + hi) >> 1)) ? 1 : 0;
+  }
 }
 
 constexpr int kPtThreads = 256;
@@ -207,13 +213,13 @@ __global__ void part_count_kernel(int l, int N, const uint32_t *__restrict__ lis
   const int j0 = blockIdx.x * kPtTile + threadIdx.x * kPtItems;
   int sp[kPtItems];
   uint8_t inl[kPtItems];  // j <= mid of its node
+  int lo = 0, hi = -1, k = 0;  // the node of the last item; descend again past its end
   for (int i = 0; i < kPtItems; ++i) {
     const int j = j0 + i;
     sp[i] = -1;
     inl[i] = 0;
     if (j < N) {
-      int lo, hi;
-      const int k = descend(j, l, N, &lo, &hi);
+      if (j > hi) k = descend(j, l, N, &lo, &hi);
       sp[i] = split[k];
       inl[i] = j <= ((lo + hi) >> 1) ? 1 : 0;
     }
@@ -248,11 +254,11 @@ __global__ void part_scatter_kernel(int l, int N, const uint32_t *__restrict__ l
   __shared__ int s_warp[33];
   int j0 = blockIdx.x * kPtTile + threadIdx.x * kPtItems;
   int lo_[kPtItems], mid_[kPtItems], hi_[kPtItems], kk_[kPtItems];
+  int lo = 0, hi = -1, k = 0;  // the node of the last item; descend again past its end
   for (int i = 0; i < kPtItems; ++i) {
     int j = j0 + i;
     if (j < N) {
-      int lo, hi;
-      int k = descend(j, l, N, &lo, &hi);
+      if (j > hi) k = descend(j, l, N, &lo, &hi);
       lo_[i] = lo;
       hi_[i] = hi;
       mid_[i] = (lo + hi) >> 1;
@@ -785,7 +791,7 @@ int build_tree(Ctx *ctx, const double *d_pos, int64_t N64, int64_t N0, const dou
     FMM_TRY(ctx->check_launch("node_kernel"));
     if (l == ml) break;
     FMM_TRY(exclusive_scan_i32(ctx, half + (cnt_level - 1), nodebase, cnt_level, nullptr));
-    flag_kernel<<<ceil_div(N, TB), TB, 0, ctx->stream>>>(l, N, lists, split, flag);
+    flag_kernel<<<ceil_div(N, TB * kFlagItems), TB, 0, ctx->stream>>>(l, N, lists, split, flag);
     part_count_kernel<<<ntiles, kPtThreads, 0, ctx->stream>>>(l, N, lists, flag, split, ntiles, tcount, fa, fs);
     FMM_TRY(ctx->check_launch("flag/part_count kernels", 2));
     FMM_TRY(exclusive_scan_i32(ctx, tcount, toff, 3 * (int64_t)ntiles, nullptr));
