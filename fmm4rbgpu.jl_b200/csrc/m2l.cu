@@ -23,16 +23,18 @@
 // are added into per-thread FP64 sums held in shared memory.
 //
 // Mixed form on the tensor cores (m2l_tc_kernel, degree n <= 4, eta <= 1/2; an
-// opt-in engine -- at n = 4 it measures ~110 ms against ~99 ms for the packed
-// CUDA-core kernel on 2^24 particles: the per-chunk hand-off between the four
-// evaluating warps and the MMA issuer costs more than the 10 FMAs per
-// evaluation it removes, and rsqrt throughput bounds both): per source the
+// opt-in engine -- at n = 4 the M2L stage measures 102 ms against 95 ms for the
+// packed CUDA-core kernel on 2^24 particles: the tensor cores take only the 71 %
+// of the pairs whose factored sums are accurate, the CUDA-core kernel still runs
+// the rest, and the per-chunk hand-off between the evaluating warps and the MMA
+// issuer keeps the rsqrt pipe at about a third of its rate): per source the
 // M2L is a (target nodes) x (source nodes) kernel matrix K times the 10 packed
 // per-source-node columns V below, so the 10 accumulations per evaluation run
 // as tcgen05 TF32 MMAs.  Each thread owns one target node = one TMEM lane: it
-// evaluates its row of K (3 FP32 ops for the denominator, rsqrt, 2 for s^3) in
-// chunks of 16 source nodes, splits every value into TF32 hi + lo and stores
-// both into a TMEM A buffer (three in rotation); one thread issues the MMAs
+// evaluates its row of K two source nodes per packed FP32x2 instruction (3 for
+// the denominator, rsqrt, 2 for s^3) in chunks of 16 source nodes, splits every
+// value into TF32 hi + lo and stores both into a TMEM A buffer (three in
+// rotation); one thread issues the MMAs
 // D += [K_hi; K_lo] x [V_hi | V_lo] (M = 128, N = 32, K = 8) against V held in
 // shared memory.  After each source D is read back (tcgen05.ld), its four
 // hi/lo products are summed and E = x'G - Q, B = W x x' - V is folded into
@@ -445,19 +447,22 @@ __global__ void __launch_bounds__(M2LShape2<NDEG>::BT)
 }
 
 // ---------------------------------------------------------------- tensor-core mixed form
-// The K dimension (source nodes) is ordered by x-rows: row r = bj + M bk holds
-// the M nodes bi = 0..M-1, and a 16-column chunk holds RPC = 16 / M whole rows
-// (column 16 c + M i + bi for row r = RPC c + i; the remaining columns are zero
-// padding).  A thread then forms the y/z part of the denominator once per row.
+// The K dimension (source nodes) is ordered for packed FP32x2 evaluation.  Node b lies
+// on x-row r = b / M = bj + M bk at bi = b % M.  The rows are paired (2 rp, 2 rp + 1), and
+// column 2 q + lane with q = M rp + bi holds row 2 rp + lane at bi.  One packed
+// evaluation then forms both columns of a pair: the two lanes share bi (the hoisted
+// x-parts of the denominator) and take their rows' y/z parts.  A row past the last
+// (M^2 odd) and the columns past 2 M NRP are zero in V.
 template <int NDEG>
 struct M2LShapeTC {
   static constexpr int M = NDEG + 1;
   static constexpr int NN = M * M * M;                 // <= 125
   static constexpr int NS = ((3 * M) + 1) & ~1;
   static constexpr int CH = 16;                        // K columns per chunk (one tcgen05.st.x16)
-  static constexpr int RPC = CH / M;                   // whole x-rows per chunk
   static constexpr int NR = M * M;                     // x-rows
-  static constexpr int NCH = (NR + RPC - 1) / RPC;
+  static constexpr int NRP = (NR + 1) / 2;             // row pairs
+  static constexpr int NQ = M * NRP;                   // packed column pairs
+  static constexpr int NCH = (2 * NQ + CH - 1) / CH;
   static constexpr int KP = NCH * CH;                  // padded K
   static constexpr int NBUF = 3;                       // TMEM A buffers in rotation
   static constexpr int NMMA = 32;                      // D columns: 0..9 V_hi products, 16..25 V_lo
@@ -467,11 +472,11 @@ struct M2LShapeTC {
   static constexpr int MOM_BYTES = 4 * NN * 4;
   static constexpr int REC = MOM_BYTES + NS * 8;       // raw FP32 moments then node coordinates
   static constexpr int SMEM_USED = 2 * BBYTES + 2 * REC;
-  // at most 4 CTAs per SM, so that 4 x 128 TMEM columns never exceed the SM's 512
+  // at most 4 CTAs per SM (3 by registers), so that 4 x 128 TMEM columns never exceed the SM's 512
   static constexpr int SMEM = SMEM_USED > 48 * 1024 ? SMEM_USED : 48 * 1024;
   static constexpr uint32_t TMEM_COLS = 128;           // D [0,32), A buffer b at 32 + 32 b (hi 16, lo 16)
   __host__ __device__ static constexpr int col(int b) {
-    return CH * ((b / M) / RPC) + M * ((b / M) % RPC) + b % M;
+    return 2 * (M * ((b / M) / 2) + b % M) + (b / M) % 2;
   }
 };
 
@@ -485,17 +490,18 @@ struct M2LShapeTC {
 constexpr int kTcThreads = 160;
 
 template <int NDEG>
-__global__ void __launch_bounds__(kTcThreads, 4)
+// Three CTAs per SM: 125 registers without spills (a bound of four spilled and ran 9 % slower).
+__global__ void __launch_bounds__(kTcThreads, 3)
     m2l_tc_kernel(const int *__restrict__ ptr, const int *__restrict__ src, const double *__restrict__ nodes,
                   const double *__restrict__ bbox, const float *__restrict__ mom, float *__restrict__ loc,
                   const double *__restrict__ consts, int accumulate, int *__restrict__ status) {
   using S = M2LShapeTC<NDEG>;
-  constexpr int M = S::M, NN = S::NN, NS = S::NS, CH = S::CH, RPC = S::RPC, NR = S::NR, NCH = S::NCH;
+  constexpr int M = S::M, NN = S::NN, NS = S::NS, CH = S::CH, NR = S::NR, NQ = S::NQ, NCH = S::NCH;
   constexpr int NBUF = S::NBUF, REC = S::REC, MOM_BYTES = S::MOM_BYTES;
   constexpr uint32_t LBO = S::LBO, SBO = S::SBO;
   constexpr uint32_t IDESC = idesc_tf32(128, S::NMMA);
   constexpr int kEvalBar = 1;  // named barrier of the 128 evaluating threads
-  static_assert(NN <= 128 && RPC >= 1, "one target node per TMEM lane, whole rows per chunk");
+  static_assert(NN <= 128 && 2 * NQ <= S::KP, "one target node per TMEM lane, every column pair in a chunk");
   extern __shared__ __align__(1024) unsigned char smem[];
   unsigned char *sRaw = smem + 2 * S::BBYTES;  // 2 raw source records (TMA double buffer)
   __shared__ __align__(8) uint64_t bar_tma[2];
@@ -663,13 +669,18 @@ __global__ void __launch_bounds__(kTcThreads, 4)
           issue(issued, issued & 1);
           ++issued;
         }
-        float prx[M], rx2[M];
+        // the x-parts of the denominator per bi (both lanes), the y/z offsets per row
+        float2 prx[M], rx2[M];
+        float ryv[M], rzv[M];
 #pragma unroll
-        for (int bi = 0; bi < M; ++bi) {
-          const float rx = xa - sn[bi];
-          prx[bi] = px * rx;
-          rx2[bi] = rx * rx;
+        for (int b = 0; b < M; ++b) {
+          const float rx = xa - sn[b];
+          prx[b] = dup2(px * rx);
+          rx2[b] = dup2(rx * rx);
+          ryv[b] = ya - sn[M + b];
+          rzv[b] = za - sn[2 * M + b];
         }
+        const float2 py2 = dup2(py), pz2 = dup2(pz), eps2 = dup2(eps);
 #pragma unroll
         for (int c = 0; c < NCH; ++c) {
           const int bsel = g % NBUF;
@@ -679,27 +690,26 @@ __global__ void __launch_bounds__(kTcThreads, 4)
           }
           uint32_t kh[CH], kl[CH];
 #pragma unroll
-          for (int j = RPC * M; j < CH; ++j) kh[j] = kl[j] = 0u;
-#pragma unroll
-          for (int ir = 0; ir < RPC; ++ir) {
-            const int r = RPC * c + ir;
-            if (r < NR) {
-              const float ry = ya - sn[M + r % M], rz = za - sn[2 * M + r / M];
-              const float P = fmaf(py, ry, pz * rz);
-              const float A = fmaf(ry, ry, fmaf(rz, rz, eps));
-#pragma unroll
-              for (int bi = 0; bi < M; ++bi) {
-                const float tt = P + prx[bi];
-                const float d = fmaf(tt, tt, A + rx2[bi]);
-                const float sv = rsqrt_approx_f32(d);
-                const float kv = (sv * sv) * sv;
-                const float h = tf32_hi(kv);
-                kh[M * ir + bi] = __float_as_uint(h);
-                kl[M * ir + bi] = __float_as_uint(kv - h);
-              }
+          for (int m = 0; m < CH / 2; ++m) {
+            const int q = (CH / 2) * c + m;  // column pair: rows 2 rp, 2 rp + 1 at bi
+            if (q < NQ) {
+              const int rp = q / M, bi = q % M;
+              const int r0 = 2 * rp, r1 = 2 * rp + 1 < NR ? 2 * rp + 1 : 2 * rp;  // a missing row repeats r0
+              const float2 ry = make_float2(ryv[r0 % M], ryv[r1 % M]), rz = make_float2(rzv[r0 / M], rzv[r1 / M]);
+              const float2 P = fma2(py2, ry, mul2(pz2, rz));
+              const float2 A = fma2(ry, ry, fma2(rz, rz, eps2));
+              const float2 tt = add2(P, prx[bi]);
+              const float2 d = fma2(tt, tt, add2(A, rx2[bi]));
+              const float2 sv = rsqrt2(d);
+              const float2 kv = mul2(mul2(sv, sv), sv);
+              const float2 h = make_float2(tf32_hi(kv.x), tf32_hi(kv.y));
+              const float2 lo = sub2(kv, h);
+              kh[2 * m] = __float_as_uint(h.x);
+              kh[2 * m + 1] = __float_as_uint(h.y);
+              kl[2 * m] = __float_as_uint(lo.x);
+              kl[2 * m + 1] = __float_as_uint(lo.y);
             } else {
-#pragma unroll
-              for (int bi = 0; bi < M; ++bi) kh[M * ir + bi] = kl[M * ir + bi] = 0u;
+              kh[2 * m] = kh[2 * m + 1] = kl[2 * m] = kl[2 * m + 1] = 0u;
             }
           }
           // the previous source's D, before this source's first chunk lets the MMAs overwrite it
