@@ -337,7 +337,33 @@ constexpr int kStCap = 4096;
 constexpr int kStThreads = 256;
 constexpr int kStItems = kStCap / kStThreads;
 constexpr int kStMaxSub = 512;    // sub-nodes of one level that split (depth <= 9)
-constexpr int kStSmem = 2 * 3 * kStCap * 2 + kStCap * 4 + kStCap * 4 + kStCap;
+constexpr int kStSmem = 2 * 3 * kStCap * 2 + kStCap * 4 + 3 * kStCap * 2 + kStCap;
+
+// Exclusive block-wide prefix sum of 64-bit values.  s_w: 33 words of shared memory; the
+// caller orders any later reuse of s_w after a barrier.
+__device__ __forceinline__ uint64_t block_excl_scan_u64(uint64_t v, uint64_t *s_w) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  uint64_t inc = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint64_t t = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += t;
+  }
+  if (lane == 31) s_w[wid] = inc;
+  __syncthreads();
+  if (wid == 0) {
+    const uint64_t w = lane < nw ? s_w[lane] : 0ull;
+    uint64_t wi = w;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint64_t t = __shfl_up_sync(0xffffffffu, wi, o);
+      if (lane >= o) wi += t;
+    }
+    if (lane < nw) s_w[lane] = wi - w;
+  }
+  __syncthreads();
+  return s_w[wid] + inc - v;
+}
 
 // Range of sub-node s (left to right) `depth` levels below [lo0, hi0].
 __device__ __forceinline__ void sub_range(int lo0, int hi0, int depth, int s, int *lo, int *hi) {
@@ -381,9 +407,9 @@ __global__ void __launch_bounds__(kStThreads)
   extern __shared__ __align__(16) unsigned char smem[];
   uint16_t *Lbuf = (uint16_t *)smem;                             // [2][3][kStCap] local ids
   uint32_t *gid = (uint32_t *)(smem + 2 * 3 * kStCap * 2);       // local id -> particle id
-  int *scan = (int *)(gid + kStCap);                             // left flags before each position
-  uint8_t *flag = (uint8_t *)(scan + kStCap);                    // left flag per local id
-  __shared__ int s_warp[33];
+  uint16_t *scan = (uint16_t *)(gid + kStCap);                   // [3][kStCap] left flags before each position
+  uint8_t *flag = (uint8_t *)(scan + 3 * kStCap);                // left flag per local id
+  __shared__ uint64_t s_warp64[33];
   __shared__ int s_split[kStMaxSub], s_mid[kStMaxSub];
   const int tid = threadIdx.x;
   const int k0 = (1 << L0) - 1 + blockIdx.x;
@@ -450,40 +476,52 @@ __global__ void __launch_bounds__(kStThreads)
       flag[L(cur, s_split[s])[p]] = (lo0 + p <= s_mid[s]) ? 1 : 0;
     }
     __syncthreads();
+    // the three lists' flags at this thread's positions as bit masks, their counts packed in
+    // 16-bit fields (a node holds at most kStCap < 2^16), one block scan for all three
+    const int b0 = tid * kStItems;
+    uint32_t fm[3];
+    uint64_t c = 0;
+#pragma unroll
     for (int a = 0; a < 3; ++a) {
-      const int b0 = tid * kStItems;
-      uint8_t f[kStItems];
-      int c = 0;
+      uint32_t m = 0;
 #pragma unroll
       for (int i = 0; i < kStItems; ++i) {
         const int p = b0 + i;
-        f[i] = p < cnt ? flag[L(cur, a)[p]] : 0;
-        c += f[i];
+        if (p < cnt && flag[L(cur, a)[p]]) m |= 1u << i;
       }
-      int ex = block_excl_scan(c, s_warp, nullptr);
+      fm[a] = m;
+      c |= (uint64_t)__popc(m) << (16 * a);
+    }
+    const uint64_t ex = block_excl_scan_u64(c, s_warp64);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      int run = (int)((ex >> (16 * a)) & 0xFFFFu);
 #pragma unroll
       for (int i = 0; i < kStItems; ++i) {
         const int p = b0 + i;
-        if (p < cnt) scan[p] = ex;
-        ex += f[i];
+        if (p < cnt) scan[a * kStCap + p] = (uint16_t)run;
+        run += (fm[a] >> i) & 1u;
       }
-      __syncthreads();
+    }
+    __syncthreads();
 #pragma unroll
-      for (int i = 0; i < kStItems; ++i) {
-        const int p = b0 + i;
-        if (p < cnt) {
-          int lo, hi;
-          const int s = sub_of(lo0, hi0, depth, lo0 + p, &lo, &hi);
-          const int lb = scan[p] - scan[lo - lo0];  // left flags before p inside its node
-          const int dest = f[i] ? lo + lb : s_mid[s] + 1 + ((lo0 + p - lo) - lb);
+    for (int i = 0; i < kStItems; ++i) {
+      const int p = b0 + i;
+      if (p < cnt) {
+        int lo, hi;
+        const int s = sub_of(lo0, hi0, depth, lo0 + p, &lo, &hi);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          const int lb = (int)scan[a * kStCap + p] - (int)scan[a * kStCap + lo - lo0];  // left flags before p in its node
+          const int dest = ((fm[a] >> i) & 1u) ? lo + lb : s_mid[s] + 1 + ((lo0 + p - lo) - lb);
           if (dest < lo || dest > hi)  // stays inside the node by construction
             atomicExch(status, kDevBadIndex);
           else
             L(cur ^ 1, a)[dest - lo0] = L(cur, a)[p];
         }
       }
-      __syncthreads();
     }
+    __syncthreads();
     cur ^= 1;
   }
   // leaves: particle ids in ascending order
