@@ -149,3 +149,75 @@ def test_gloo_ranks_partition_like_the_oracle(tmp_path, counts):
         assert gathered == [[10 * k + i for i in range(k + 1)] for k in range(world)]
         assert a2a == [[100 * k + r] * (r + 1) for k in range(world)]
         assert red == [float(world - 1), 0.0]
+
+
+def _brute_local(g, L, ml, rank, remote):
+    """Local cluster number of global heap id g on `rank`, by walking the tree."""
+    lev = (g + 1).bit_length() - 1
+    nc_sub = (2 << (ml - L)) - 1
+    ntop = (2 << L) - 1
+    a = g
+    while (a + 1).bit_length() - 1 > L:
+        a = (a - 1) // 2
+    owner = a - ((1 << L) - 1) if lev >= L else -1
+    if owner == rank:
+        d = lev - L
+        return (1 << d) - 1 + (g - ((1 << lev) - 1) - (rank << d))
+    if lev <= L:
+        return nc_sub + g
+    return nc_sub + ntop + remote.index(g)
+
+
+@pytest.mark.parametrize("L,ml,rank", [(1, 4, 0), (2, 5, 1), (3, 6, 6)])
+def test_local_numbering_and_local_csr_match_a_tree_walk(L, ml, rank):
+    """_Plan.local: a rank's own subtree first (heap order, its level-L root at 0), then the whole
+    tree's top 2^(L+1) - 1 clusters (nc_sub + heap id), then the remote clusters in ascending
+    global id.
+    _csr_to_local keeps every row's source order and orders rows by local target."""
+    import torch
+
+    from fmmb200 import sharded
+
+    rng = np.random.default_rng(L * 100 + rank)
+    nc = (2 << ml) - 1
+    levels = np.floor(np.log2(np.arange(nc) + 1)).astype(int)
+    g_root = (1 << L) - 1 + rank
+
+    def mine_or_ancestor(t):
+        a = t
+        while a > g_root:
+            a = (a - 1) // 2
+        b = g_root
+        while b > t:
+            b = (b - 1) // 2
+        return a == g_root or b == t
+
+    targets = [t for t in range(nc) if mine_or_ancestor(t)]
+    rows = {t: sorted(rng.choice(nc, size=rng.integers(0, 6), replace=False).tolist()) for t in targets}
+    ptr = np.zeros(nc + 1, np.int64)
+    for t in range(nc):
+        ptr[t + 1] = ptr[t] + len(rows.get(t, []))
+    src = np.array([s for t in range(nc) for s in rows.get(t, [])], np.int64)
+    below = sorted({int(s) for s in src if levels[s] > L})
+    remote = [s for s in below if ((s + 1) >> (levels[s] - L)) - 1 != g_root]  # outside the own subtree
+    plan = sharded._Plan(L, ml, rank, torch.tensor(remote, dtype=torch.int64))
+    every = [t for t in range(nc) if levels[t] <= L or ((t + 1) >> (levels[t] - L)) - 1 == g_root] + remote
+    got = plan.local(torch.tensor(every, dtype=torch.int64)).tolist()
+    want = [_brute_local(g, L, ml, rank, remote) for g in every]
+    assert got == want
+    nc_loc = plan.nc_sub + plan.ntop + len(remote)
+    # every local number once, except the top part's slot of the rank's own root: the top levels
+    # keep every level-L root's moments there (a contiguous heap for their M2M), while the
+    # own root's rows live at local 0
+    assert sorted(want) == [x for x in range(nc_loc) if x != plan.nc_sub + g_root]
+    lptr, lsrc = sharded._csr_to_local(plan, torch.tensor(ptr, dtype=torch.int32), torch.tensor(src, dtype=torch.int32),
+                                       nc_loc)
+    lrows = {}
+    for t in targets:
+        lrows[_brute_local(t, L, ml, rank, remote)] = [_brute_local(s, L, ml, rank, remote) for s in rows[t]]
+    wptr = np.zeros(nc_loc + 1, np.int64)
+    for lt in range(nc_loc):
+        wptr[lt + 1] = wptr[lt] + len(lrows.get(lt, []))
+    wsrc = [s for lt in range(nc_loc) for s in lrows.get(lt, [])]
+    assert lptr.tolist() == wptr.tolist()
+    assert lsrc.tolist() == wsrc
