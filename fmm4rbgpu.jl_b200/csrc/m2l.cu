@@ -769,7 +769,6 @@ template <int M>
 __global__ void m2l_split_count_kernel(int64_t nc, const int *__restrict__ ptr, const int *__restrict__ src,
                                        const double *__restrict__ nodes, const double *__restrict__ bbox,
                                        int *__restrict__ cnt) {
-  constexpr int NS = ((3 * M) + 1) & ~1;
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t > nc) return;
   int a = 0, b = 0;
@@ -791,7 +790,6 @@ template <int M>
 __global__ void m2l_split_write_kernel(int64_t nc, const int *__restrict__ ptr, const int *__restrict__ src,
                                        const double *__restrict__ nodes, const double *__restrict__ bbox,
                                        const int *__restrict__ ptr2, int *__restrict__ src_a, int *__restrict__ src_b) {
-  constexpr int NS = ((3 * M) + 1) & ~1;
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nc) return;
   const double *tb = bbox + 6 * t;
