@@ -29,6 +29,8 @@ constexpr int kTvItems = 4;
 constexpr int kTvTile = kTvThreads * kTvItems;
 
 enum : int { kCatP2P = 0, kCatM2L = 1, kCatSplit = 2 };
+// per-pair codes the count kernel leaves for the write kernel (kCatP2P and kCatM2L as above)
+enum : int { kCodeSplitT = 2, kCodeSplitS = 3 };
 
 // Target filter of a sharded traversal (TravFilter::L < 0: every target).  A rank that
 // owns the level-L cluster g (heap id) needs the rows of g's descendants and of g's
@@ -81,7 +83,8 @@ __device__ __forceinline__ int classify(const ClusterGeom *__restrict__ geom, in
 // strides over the tiles that the frontier (state, on the device) occupies.
 __global__ void trav_count_kernel(const int2 *__restrict__ front, const long long *__restrict__ state,
                                   const ClusterGeom *__restrict__ geom, const double *__restrict__ consts, double eta,
-                                  int nblk, TravFilter flt, int *__restrict__ bcount, int *__restrict__ totals) {
+                                  int nblk, TravFilter flt, int *__restrict__ bcount, int *__restrict__ totals,
+                                  uint8_t *__restrict__ code) {
   __shared__ int s_warp[33];
   const int nf = (int)state[kTsFront];
   const int ntile = (nf + kTvTile - 1) / kTvTile;
@@ -99,6 +102,8 @@ __global__ void trav_count_kernel(const int2 *__restrict__ front, const long lon
           c[2] += (int)trav_relevant(a, flt) + (int)trav_relevant(cc, flt);
         else
           c[cat]++;
+        // the decision for trav_write_kernel: P2P, M2L, split the target, split the source
+        code[q] = (uint8_t)(cat != kCatSplit ? cat : (a != p.x ? kCodeSplitT : kCodeSplitS));
       }
     }
     for (int k = 0; k < 3; ++k) {
@@ -146,18 +151,16 @@ __global__ void __launch_bounds__(1024) tile_scan_kernel(const int *__restrict__
 }
 
 // Writes the step's pairs after the ones of the earlier steps (state) and its children as
-// the next frontier; a write past a buffer's capacity is dropped (the step's totals still
+// the next frontier, from the count kernel's decision per pair (no geometry is read again); a write past a buffer's capacity is dropped (the step's totals still
 // count it, and trav_advance_kernel raises the overflow flag).
 __global__ void trav_write_kernel(const int2 *__restrict__ front, const long long *__restrict__ state,
-                                  const ClusterGeom *__restrict__ geom, const double *__restrict__ consts, double eta,
-                                  int nblk, TravFilter flt, const int *__restrict__ boff, int bits,
-                                  uint64_t *__restrict__ p2p, long long cap_p, uint64_t *__restrict__ m2l,
-                                  long long cap_m, int2 *__restrict__ next, long long cap_f) {
+                                  const uint8_t *__restrict__ code, int nblk, TravFilter flt,
+                                  const int *__restrict__ boff, int bits, uint64_t *__restrict__ p2p, long long cap_p,
+                                  uint64_t *__restrict__ m2l, long long cap_m, int2 *__restrict__ next, long long cap_f) {
   __shared__ int s_warp[33];
   const int nf = (int)state[kTsFront];
   const int ntile = (nf + kTvTile - 1) / kTvTile;
   const long long base_p = state[kTsP2P], base_m = state[kTsM2L];
-  const double s0 = consts[3], s1 = consts[4], s2 = consts[5];
   for (int tile = blockIdx.x; tile < ntile; tile += gridDim.x) {
     int cat[kTvItems];
     int2 pr[kTvItems], ch1[kTvItems], ch2[kTvItems];
@@ -168,7 +171,15 @@ __global__ void trav_write_kernel(const int2 *__restrict__ front, const long lon
       cat[i] = -1;
       if (q < nf) {
         pr[i] = front[q];
-        cat[i] = classify(geom, pr[i].x, pr[i].y, s0, s1, s2, eta, &ch1[i].x, &ch1[i].y, &ch2[i].x, &ch2[i].y);
+        const int k = code[q];  // the count kernel's decision for this pair
+        cat[i] = k < kCatSplit ? k : kCatSplit;
+        if (k == kCodeSplitT) {
+          ch1[i] = make_int2(2 * pr[i].x + 1, pr[i].y);
+          ch2[i] = make_int2(2 * pr[i].x + 2, pr[i].y);
+        } else if (k == kCodeSplitS) {
+          ch1[i] = make_int2(pr[i].x, 2 * pr[i].y + 1);
+          ch2[i] = make_int2(pr[i].x, 2 * pr[i].y + 2);
+        }
         if (cat[i] == kCatSplit)
           c[2] += (int)trav_relevant(ch1[i].x, flt) + (int)trav_relevant(ch2[i].x, flt);
         else
@@ -477,6 +488,8 @@ int build_lists(Ctx *ctx, double eta, const double *d_consts) {
     const int grid = nblk < 148 * 8 ? nblk : 148 * 8;       // blocks, striding over the tiles in use
     FMM_TRY(ctx->ensure("trav_bcount", 3 * (int64_t)nblk, &bcount));
     FMM_TRY(ctx->ensure("trav_boff", 3 * (int64_t)nblk, &boff));
+    uint8_t *code;
+    FMM_TRY(ctx->ensure("trav_code", cap_f, &code));  // one decision per frontier pair
     const long long init[kTsWords] = {1, 0, 0, 0, 1, 0, 0, 0};
     const int2 root = make_int2(0, 0);
     FMM_CUDA_TRY(ctx, cudaMemcpyAsync(state, init, sizeof(init), cudaMemcpyHostToDevice, ctx->stream));
@@ -486,10 +499,10 @@ int build_lists(Ctx *ctx, double eta, const double *d_consts) {
       const int2 *cur = step % 2 == 0 ? fa : fb;
       int2 *nxt = step % 2 == 0 ? fb : fa;
       trav_count_kernel<<<grid, kTvThreads, 0, ctx->stream>>>(cur, state, geom, d_consts, eta, nblk, flt, bcount,
-                                                               totals);
+                                                               totals, code);
       tile_scan_kernel<<<1, 1024, 0, ctx->stream>>>(bcount, nblk, state, boff);
-      trav_write_kernel<<<grid, kTvThreads, 0, ctx->stream>>>(cur, state, geom, d_consts, eta, nblk, flt, boff, bits,
-                                                               p2p, cap_p, m2l, cap_m, nxt, cap_f);
+      trav_write_kernel<<<grid, kTvThreads, 0, ctx->stream>>>(cur, state, code, nblk, flt, boff, bits, p2p, cap_p, m2l,
+                                                               cap_m, nxt, cap_f);
       trav_advance_kernel<<<1, 32, 0, ctx->stream>>>(state, totals, cap_p, cap_m, cap_f);
       FMM_TRY(ctx->check_launch("trav_count/scan/write/advance kernels", 4));
     }
