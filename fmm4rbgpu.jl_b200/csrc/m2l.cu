@@ -239,7 +239,8 @@ template <int NDEG, bool MASK>
 __global__ void __launch_bounds__(M2LShape2<NDEG>::BT)
     m2l_x2_kernel(const int *__restrict__ ptr, const int *__restrict__ src, const double *__restrict__ nodes,
                   const double *__restrict__ bbox, const float *__restrict__ mom, float *__restrict__ loc,
-                  const double *__restrict__ consts, int accumulate, int *__restrict__ status) {
+                  const double *__restrict__ consts, int accumulate, int *__restrict__ status,
+                  const uint32_t *__restrict__ srcf) {
   using S = M2LShape2<NDEG>;
   constexpr int M = S::M, NN = S::NN, NS = S::NS, NP = S::NP, TPP = S::TPP, BT = S::BT, REC = S::REC;
   constexpr int MOM_BYTES = 4 * NN * 4;
@@ -273,12 +274,21 @@ __global__ void __launch_bounds__(M2LShape2<NDEG>::BT)
     }
     __syncthreads();
     auto issue = [&](int k, int bb) {
-      const int s = src[p0 + k];
-      unsigned char *dst = smem + bb * REC;
       // factored sums unless the two boxes nearly touch (factored_ok); at N = 2^24 the
-      // direct pairs make the M2L about 2 % slower and its error ~20x smaller.  Written
-      // before the arrive, whose release orders it for the threads that wait on bar[bb].
-      s_dir[bb] = MASK || !factored_ok(bbox + 6 * (int64_t)s, tb, cx, cy, cz);
+      // direct pairs make the M2L about 2 % slower and its error ~20x smaller.  srcf, when
+      // given, holds the source with that decision in its top bit (m2l_dirflag_kernel), so
+      // that this thread does not evaluate it between its own sweeps.  Written before the
+      // arrive, whose release orders it for the threads that wait on bar[bb].
+      int s;
+      if (srcf) {
+        const uint32_t v = srcf[p0 + k];
+        s = (int)(v & 0x7FFFFFFFu);
+        s_dir[bb] = MASK || (v >> 31) != 0u;
+      } else {
+        s = src[p0 + k];
+        s_dir[bb] = MASK || !factored_ok(bbox + 6 * (int64_t)s, tb, cx, cy, cz);
+      }
+      unsigned char *dst = smem + bb * REC;
       mbar_arrive_expect_tx(&bar[bb], REC);
       bulk_g2s(dst, mom + (int64_t)s * 4 * NN, MOM_BYTES, &bar[bb]);
       bulk_g2s(dst + MOM_BYTES, nodes + (int64_t)s * NS, NS * 8, &bar[bb]);
@@ -443,6 +453,20 @@ __global__ void __launch_bounds__(M2LShape2<NDEG>::BT)
         }
       }
     }
+  }
+}
+
+// srcf[k] = src[k] with the top bit set when target t's pair with it takes the direct sums
+// (factored_ok false), for every row t of the CSR lists; one thread per target.
+__global__ void m2l_dirflag_kernel(int64_t nc, const int *__restrict__ ptr, const int *__restrict__ src,
+                                   const double *__restrict__ bbox, uint32_t *__restrict__ srcf) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nc) return;
+  const double *tb = bbox + 6 * t;
+  const double cx = 0.5 * (tb[0] + tb[3]), cy = 0.5 * (tb[1] + tb[4]), cz = 0.5 * (tb[2] + tb[5]);
+  for (int k = ptr[t]; k < ptr[t + 1]; ++k) {
+    const int s = src[k];
+    srcf[k] = (uint32_t)s | (factored_ok(bbox + 6 * (int64_t)s, tb, cx, cy, cz) ? 0u : 0x80000000u);
   }
 }
 
@@ -837,7 +861,7 @@ int launch_m2l_tc(Ctx *ctx, bool accumulate) {
   FMM_TRY(opt_in_smem(ctx, k2, S2::SMEM));
   k2<<<(unsigned)nc, S2::BT, S2::SMEM, ctx->stream>>>(ptr2 + nc + 1, src_b, nodes, bbox, ctx->get<float>("mom32"),
                                                       ctx->get<float>("loc32"), ctx->get<double>("consts"), 1,
-                                                      ctx->d_status);
+                                                      ctx->d_status, nullptr);
   return ctx->check_launch("m2l_x2_kernel");
 }
 
@@ -851,11 +875,17 @@ int launch_m2l_mixed(Ctx *ctx, bool accumulate) {
   using S = M2LShape2<NDEG>;
   auto kern = m2l_x2_kernel<NDEG, MASK>;
   FMM_TRY(opt_in_smem(ctx, kern, S::SMEM));
+  const int *ptr = ctx->get<int>(ctx->m2l_ptr_key), *src = ctx->get<int>(ctx->m2l_src_key);
+  uint32_t *srcf = nullptr;
+  if (!MASK && ctx->nc > 0 && ctx->nm2l > 0) {  // every pair's factored / direct decision, up front
+    FMM_TRY(ctx->ensure("m2l_srcf", ctx->nm2l, &srcf));
+    m2l_dirflag_kernel<<<ceil_div(ctx->nc, 128), 128, 0, ctx->stream>>>(ctx->nc, ptr, src, ctx->get<double>("bbox"), srcf);
+    FMM_TRY(ctx->check_launch("m2l_dirflag_kernel"));
+  }
   if (ctx->nc > 0)
     kern<<<(unsigned)ctx->nc, S::BT, S::SMEM, ctx->stream>>>(
-        ctx->get<int>(ctx->m2l_ptr_key), ctx->get<int>(ctx->m2l_src_key), ctx->get<double>("nodes"), ctx->get<double>("bbox"),
-        ctx->get<float>("mom32"), ctx->get<float>("loc32"), ctx->get<double>("consts"), accumulate ? 1 : 0,
-        ctx->d_status);
+        ptr, src, ctx->get<double>("nodes"), ctx->get<double>("bbox"), ctx->get<float>("mom32"), ctx->get<float>("loc32"),
+        ctx->get<double>("consts"), accumulate ? 1 : 0, ctx->d_status, srcf);
   return ctx->check_launch("m2l_x2_kernel");
 }
 
